@@ -1,0 +1,164 @@
+"""ctypes binding of libbcc.so, the CUDA checker (C ABI in include/bcc.h).
+
+``Checker`` mirrors the reference operator batch_cc::batch_cc<Robot>
+(src/batch_cc.hh:4-6, src/batch_cc.cu:244-338): environments + edges
+[E, 2, dof] + resolution in, verdicts [E, N] out (True = in collision, layout
+[edge][env] as src/batch_cc.cu:131).  Errors raise ``BccError`` with the
+library's message, as the reference throws std::runtime_error for bad
+environments (src/batch_cc.cu:45-56).
+
+There is no CPU fallback: if libbcc.so is missing or no CUDA device is
+present, constructing a Checker raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .envs import BccEnvSoa
+
+HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(HERE, "libbcc.so")
+ROBOTS = {"panda": 0, "fetch": 1, "baxter": 2}
+ORDERS = {"plain": 0, "learned": 1}
+STATUS = {0: "BCC_OK", 1: "BCC_ERR_INVALID_ARGUMENT", 2: "BCC_ERR_CUDA", 3: "BCC_ERR_NO_ENVS",
+          4: "BCC_ERR_TIMEOUT", 5: "BCC_ERR_NOT_SUPPORTED", 6: "BCC_ERR_LIMIT"}
+
+
+class BccError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+class BccOpts(ctypes.Structure):
+    _fields_ = [("order", ctypes.c_int32), ("use_graph", ctypes.c_int32),
+                ("tile_override", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libbcc.so not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.bcc_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int]
+        L.bcc_destroy.argtypes = [vp]
+        L.bcc_destroy.restype = None
+        L.bcc_last_error.argtypes = [vp]
+        L.bcc_last_error.restype = ctypes.c_char_p
+        L.bcc_upload_envs.argtypes = [vp, ctypes.POINTER(BccEnvSoa)]
+        L.bcc_check.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
+                                ctypes.c_int32, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(BccOpts)]
+        L.bcc_check_device.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int32, ctypes.c_int32, vp,
+                                       ctypes.POINTER(BccOpts), vp]
+        L.bcc_edge_samples.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                       ctypes.c_int32, ctypes.c_int32]
+        L.bcc_robot_dof.argtypes = [ctypes.c_int]
+        L.bcc_measure_fp32_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+        L.bcc_set_profiling.argtypes = [vp, ctypes.c_int32]
+        L.bcc_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
+        L.bcc_pack_envs.argtypes = [ctypes.POINTER(BccEnvSoa), ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64),
+                                    ctypes.POINTER(ctypes.c_int32)]
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names declared in include/bcc.h (checked against the .so by the tests)."""
+    return ["bcc_create", "bcc_destroy", "bcc_last_error", "bcc_upload_envs", "bcc_check",
+            "bcc_check_device", "bcc_edge_samples", "bcc_robot_dof", "bcc_pack_envs",
+            "bcc_set_profiling", "bcc_stage_times", "bcc_measure_fp32_peak"]
+
+
+def make_opts(order="plain", use_graph=False, tile=0):
+    o = BccOpts()
+    o.order = ORDERS[order]
+    o.use_graph = int(bool(use_graph))
+    o.tile_override = int(tile)
+    return o
+
+
+class Checker:
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        st = lib().bcc_create(ctypes.byref(self._h), device)
+        if st != 0:
+            raise BccError(st, "bcc_create failed (no CUDA device?)")
+        self.num_envs = None
+
+    def close(self):
+        if self._h:
+            lib().bcc_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _raise(self, st):
+        if st != 0:
+            raise BccError(st, lib().bcc_last_error(self._h).decode())
+
+    def upload(self, envset):
+        soa = envset.as_ctypes()
+        self._raise(lib().bcc_upload_envs(self._h, ctypes.byref(soa)))
+        self.num_envs = envset.num_envs
+
+    def check(self, edges, resolution=32, robot="panda", order="plain", out=None, tile=0):
+        """Host API: edges float32 [E, 2, dof] -> verdicts uint8 [E, num_envs]."""
+        edges = np.ascontiguousarray(edges, np.float32)
+        E = edges.shape[0]
+        if out is None:
+            out = np.zeros((E, self.num_envs), np.uint8)
+        opts = make_opts(order, tile=tile)
+        st = lib().bcc_check(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                             E, resolution, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                             ctypes.byref(opts))
+        self._raise(st)
+        return out
+
+    def set_profiling(self, on=True):
+        self._raise(lib().bcc_set_profiling(self._h, int(on)))
+
+    STAGES = ("steps", "fk", "self", "swept", "check")
+
+    def stage_times(self):
+        """Device ms of the last check's stages (stream must be synchronised)."""
+        ms = (ctypes.c_float * 5)()
+        n = lib().bcc_stage_times(self._h, ms, 5)
+        if n < 0:
+            raise BccError(1, "profiling is off or no check has run")
+        return dict(zip(self.STAGES, [float(ms[i]) for i in range(n)]))
+
+    def check_device(self, d_edges_ptr, num_edges, d_results_ptr, resolution=32, robot="panda",
+                     order="plain", stream=0, tile=0):
+        """Device API: raw device pointers (e.g. torch tensors' data_ptr()), stream-ordered."""
+        opts = make_opts(order, tile=tile)
+        st = lib().bcc_check_device(self._h, ROBOTS[robot], ctypes.c_void_p(d_edges_ptr), num_edges,
+                                    resolution, ctypes.c_void_p(d_results_ptr), ctypes.byref(opts),
+                                    ctypes.c_void_p(stream))
+        self._raise(st)
+
+
+def edge_samples(start, end, resolution=32):
+    s = np.ascontiguousarray(start, np.float32)
+    e = np.ascontiguousarray(end, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    return lib().bcc_edge_samples(s.ctypes.data_as(fp), e.ctypes.data_as(fp), len(s), resolution)
+
+
+def measure_fp32_peak(device=0):
+    """FP32 FMA-pipe peak (TFLOP/s) of the device, from the library's probe kernel."""
+    t = ctypes.c_double(0)
+    st = lib().bcc_measure_fp32_peak(device, ctypes.byref(t))
+    if st != 0:
+        raise BccError(st, "fp32 peak probe failed")
+    return t.value

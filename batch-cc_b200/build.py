@@ -1,0 +1,66 @@
+"""Build the native parts in-tree (sm_100a only).
+
+* batch-cc_b200/libbcc.so  -- the product: CUDA kernels + C ABI (include/bcc.h)
+* batch-cc_b200/batch_cc   -- the drop-in CLI driver (scripts/batch_cc_mbm.cpp's
+                              `batch_cc <robot> <num_envs> <num_edges>`)
+
+Every nvcc invocation targets `-gencode arch=compute_100a,code=sm_100a`; nvcc
+cross-compiles without a GPU.  Rebuilds only when a source is newer than the
+output.
+"""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libbcc.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+           "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+
+def _newer(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def deps():
+    return sources() + sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))) + [
+        os.path.join(ROOT, "include", "bcc.h")]
+
+
+def build_lib(force=False):
+    objs = []
+    dep = deps()
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    for src in sources():
+        obj = os.path.join(HERE, "_build", os.path.basename(src) + ".o")
+        if force or _newer(obj, dep):
+            _run([NVCC] + ARCH + NVFLAGS + ["-c", src, "-o", obj])
+        objs.append(obj)
+    if force or _newer(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+    return LIB
+
+
+def build_all(force=False):
+    build_lib(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

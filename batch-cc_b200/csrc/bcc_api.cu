@@ -1,0 +1,428 @@
+// bcc_api.cu -- C ABI of the checker (include/bcc.h): context, environment
+// arena upload, and the check entry points.
+//
+// Replaces the reference host entry batch_cc::batch_cc<Robot>
+// (src/batch_cc.cu:244-338): instead of two cudaMalloc + a pinned staging blob
+// per environment and a device pointer table, all environments live in one
+// packed arena of 80-byte rounded-box records that persists across calls; the
+// per-call buffers (edges, sample table, verdicts) are grown on demand and
+// reused.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/bcc.h"
+#include "bcc_device.cuh"
+#include "bcc_kernels.h"
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        const size_t want = std::max(bytes, cap * 3 / 2);
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct bcc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool tables[3] = {false, false, false};
+    // environment arena
+    int num_envs = -1;
+    int max_prims = 0;
+    DevBuf prims, env_off;
+    // per-call buffers
+    DevBuf edges, steps, offs, table, row_edge, edge_self, swept, results, error_flag;
+    int* h_total = nullptr;  // pinned readback of the sample-row total
+    bool profiling = false;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+bcc_status fail(bcc_ctx* c, bcc_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+bcc_status cuda_fail(bcc_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, BCC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BCC_CUDA(ctx, call)                                          \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return cuda_fail((ctx), _e, #call);   \
+    } while (0)
+
+// Orthonormal pair completing unit vector a (FP64).
+void complete_basis(const double a[3], double u[3], double w[3]) {
+    double t[3] = {0, 0, 0};
+    int m = std::fabs(a[0]) <= std::fabs(a[1]) ? (std::fabs(a[0]) <= std::fabs(a[2]) ? 0 : 2)
+                                               : (std::fabs(a[1]) <= std::fabs(a[2]) ? 1 : 2);
+    t[m] = 1.0;
+    double d = t[0] * a[0] + t[1] * a[1] + t[2] * a[2];
+    for (int i = 0; i < 3; ++i) u[i] = t[i] - d * a[i];
+    double nu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    for (int i = 0; i < 3; ++i) u[i] /= nu;
+    w[0] = a[1] * u[2] - a[2] * u[1];
+    w[1] = a[2] * u[0] - a[0] * u[2];
+    w[2] = a[0] * u[1] - a[1] * u[0];
+}
+
+struct Rec {
+    float v[20];
+};
+
+// Rounded box: centre c, axes A (rows), half-extents h, rounding radius rho.
+Rec make_rec(const double c[3], const double A[3][3], const double h[3], double rho) {
+    Rec r;
+    r.v[0] = (float)c[0];
+    r.v[1] = (float)c[1];
+    r.v[2] = (float)c[2];
+    r.v[3] = (float)rho;
+    for (int i = 0; i < 3; ++i) {
+        r.v[4 + 4 * i + 0] = (float)A[i][0];
+        r.v[4 + 4 * i + 1] = (float)A[i][1];
+        r.v[4 + 4 * i + 2] = (float)A[i][2];
+        r.v[4 + 4 * i + 3] = (float)h[i];
+    }
+    // AABB half-size of the rounded box (+ cull margin), rounded outward.
+    for (int k = 0; k < 3; ++k) {
+        double hs = rho;
+        for (int i = 0; i < 3; ++i) hs += std::fabs((double)(float)A[i][k]) * h[i];
+        hs = hs * (1.0 + 1e-6) + 1e-6 + (double)bcc::kCullMargin;
+        r.v[16 + k] = (float)hs;
+    }
+    r.v[19] = 0.0f;
+    return r;
+}
+
+Rec rec_sphere(const float* s) {
+    double c[3] = {s[0], s[1], s[2]};
+    double A[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    double h[3] = {0, 0, 0};
+    return make_rec(c, A, h, s[3]);
+}
+
+// Capsule x1 y1 z1 xv yv zv r rdv: segment p1 -> p1 + v with radius r
+// (src/utils.cuh:114-127).  A zero-length segment is the sphere at p1, which is
+// what the reference's NaN clamp (rdv = inf) evaluates to.
+Rec rec_capsule(const float* k, bool z_aligned) {
+    double p1[3] = {k[0], k[1], k[2]};
+    double v[3] = {z_aligned ? 0.0 : (double)k[3], z_aligned ? 0.0 : (double)k[4], (double)k[5]};
+    double L = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double c[3], A[3][3], h[3] = {0, 0, 0};
+    double a[3] = {0, 0, 1};
+    if (L > 0) {
+        for (int i = 0; i < 3; ++i) a[i] = v[i] / L;
+        h[2] = 0.5 * L;
+    }
+    for (int i = 0; i < 3; ++i) c[i] = p1[i] + 0.5 * v[i];
+    double u[3], w[3];
+    complete_basis(a, u, w);
+    for (int i = 0; i < 3; ++i) {
+        A[0][i] = u[i];
+        A[1][i] = w[i];
+        A[2][i] = a[i];
+    }
+    return make_rec(c, A, h, k[6]);
+}
+
+// Cuboid x y z a1 a2 a3 h1 h2 h3 (src/utils.cuh:159-178); the z-aligned variant
+// projects on (a1x, a1y, 0), (a2x, a2y, 0) and (0, 0, 1) (:187-205).
+Rec rec_cuboid(const float* b, bool z_aligned) {
+    double c[3] = {b[0], b[1], b[2]};
+    double A[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) A[i][j] = b[3 + 3 * i + j];
+    if (z_aligned) {
+        A[0][2] = 0;
+        A[1][2] = 0;
+        A[2][0] = 0;
+        A[2][1] = 0;
+        A[2][2] = 1;
+    }
+    double h[3] = {b[12], b[13], b[14]};
+    return make_rec(c, A, h, 0.0);
+}
+
+int clamp_tile(int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); }
+
+bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution,
+                     uint8_t* d_results, const bcc_opts* opts, cudaStream_t st) {
+    const int r = (int)robot;
+    if (r != BCC_ROBOT_PANDA) return fail(ctx, BCC_ERR_NOT_SUPPORTED, "robot not built into this library");
+    if (!ctx->tables[r]) {
+        BCC_CUDA(ctx, bcc::upload_robot_tables(r));
+        ctx->tables[r] = true;
+    }
+    (void)opts;
+    bcc::PipelineArgs a{};
+    a.d_edges = d_edges;
+    a.num_edges = E;
+    a.resolution = resolution;
+    BCC_CUDA(ctx, ctx->steps.ensure(sizeof(int) * (size_t)E));
+    BCC_CUDA(ctx, ctx->offs.ensure(sizeof(int) * ((size_t)E + 1)));
+    BCC_CUDA(ctx, ctx->edge_self.ensure(sizeof(int) * (size_t)E));
+    const int G = bcc::robot_num_env_groups(r);
+    BCC_CUDA(ctx, ctx->swept.ensure(sizeof(float4) * 2 * (size_t)G * E));
+    BCC_CUDA(ctx, ctx->error_flag.ensure(sizeof(int)));
+    a.steps = ctx->steps.as<int>();
+    a.offs = ctx->offs.as<int>();
+    a.edge_self = ctx->edge_self.as<int>();
+    a.swept = ctx->swept.as<float4>();
+    a.error_flag = ctx->error_flag.as<int>();
+    a.stage_events = ctx->profiling ? ctx->ev : nullptr;
+    BCC_CUDA(ctx, cudaMemsetAsync(a.error_flag, 0, sizeof(int), st));
+    BCC_CUDA(ctx, bcc::launch_steps(r, a, st));
+    BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.offs + E, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    const int total = *ctx->h_total;
+    if (total < 0) return fail(ctx, BCC_ERR_LIMIT, "sample count overflows int32");
+    const int NS = bcc::robot_num_spheres(r);
+    BCC_CUDA(ctx, ctx->table.ensure(sizeof(float4) * (size_t)NS * std::max(total, 1)));
+    BCC_CUDA(ctx, ctx->row_edge.ensure(sizeof(int) * (size_t)std::max(total, 1)));
+    a.total_rows = total;
+    a.table = ctx->table.as<float4>();
+    a.row_edge = ctx->row_edge.as<int>();
+    a.prims = ctx->prims.as<float4>();
+    a.env_off = ctx->env_off.as<int>();
+    a.num_envs = ctx->num_envs;
+    a.max_prims = std::max(ctx->max_prims, 1);
+    a.d_results = d_results;
+    // Tile: warps per CTA limited by shared memory; environments per CTA.
+    int warps = 8;
+    while (warps > 1 && bcc::check_smem_bytes(a.max_prims, warps) > 200 * 1024) warps >>= 1;
+    if (bcc::check_smem_bytes(a.max_prims, warps) > 220 * 1024)
+        return fail(ctx, BCC_ERR_LIMIT, "an environment has too many primitives for shared-memory staging");
+    a.warps = warps;
+    a.envs_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : 64, 1, 1 << 20);
+    BCC_CUDA(ctx, bcc::launch_check(r, a, st));
+    return BCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+bcc_status bcc_create(bcc_ctx** out, int device) {
+    if (!out) return BCC_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    bcc_ctx* c = new bcc_ctx();
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_total, sizeof(int));
+    if (e != cudaSuccess) {
+        delete c;
+        return BCC_ERR_CUDA;
+    }
+    *out = c;
+    return BCC_OK;
+}
+
+void bcc_destroy(bcc_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->h_total) cudaFreeHost(ctx->h_total);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* bcc_last_error(const bcc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+bcc_status bcc_set_profiling(bcc_ctx* ctx, int32_t on) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    for (auto& e : ctx->ev)
+        if (!e) BCC_CUDA(ctx, cudaEventCreate(&e));
+    ctx->profiling = on != 0;
+    return BCC_OK;
+}
+
+int32_t bcc_stage_times(bcc_ctx* ctx, float* ms, int32_t max_stages) {
+    if (!ctx || !ms || !ctx->profiling) return -1;
+    int n = std::min(max_stages, 5);
+    for (int i = 0; i < n; ++i) {
+        if (cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]) != cudaSuccess) return -1;
+    }
+    return n;
+}
+
+int32_t bcc_robot_dof(bcc_robot robot) {
+    switch (robot) {
+        case BCC_ROBOT_PANDA: return 7;
+        case BCC_ROBOT_FETCH: return 8;
+        case BCC_ROBOT_BAXTER: return 14;
+        default: return -1;
+    }
+}
+
+int32_t bcc_edge_samples(const float* start, const float* end, int32_t dof, int32_t resolution) {
+    if (!start || !end || dof <= 0 || dof > 16) return -1;
+    // Host copy of the reference discretisation (src/batch_cc.cu:103-107).
+    float ans = 0.0f;
+    for (int j = 0; j < dof; ++j) {
+        float d = start[j] - end[j];
+        ans = std::fmaf(d, d, ans);
+    }
+    float dist = std::sqrt(ans);
+    float nf = std::fmax(std::ceil((dist / 31.0f) * (float)resolution), 1.0f);
+    return 32 * (int)nf;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Validation + packing shared by bcc_upload_envs and bcc_pack_envs.
+bcc_status pack(bcc_ctx* ctx, const bcc_env_soa* envs, std::vector<Rec>& recs, std::vector<int>& off,
+                int& max_prims) {
+    if (!envs || envs->num_envs < 0) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "null or negative environment set");
+    const int N = envs->num_envs;
+    const uint32_t* cnt[6] = {envs->num_spheres, envs->num_capsules, envs->num_z_capsules,
+                              envs->num_cuboids, envs->num_z_cuboids, envs->num_cylinders};
+    const float* rec[6] = {envs->spheres, envs->capsules, envs->z_capsules,
+                           envs->cuboids, envs->z_cuboids, envs->cylinders};
+    const int width[6] = {4, 8, 8, 15, 15, 8};
+    const char* names[6] = {"spheres", "capsules", "z_capsules", "cuboids", "z_cuboids", "cylinders"};
+    // ensure_ptr_count_consistent (src/batch_cc.cu:45-56): positive count needs records.
+    for (int k = 0; k < 6; ++k) {
+        if (!cnt[k]) continue;
+        size_t tot = 0;
+        for (int i = 0; i < N; ++i) tot += cnt[k][i];
+        if (tot > 0 && !rec[k])
+            return fail(ctx, BCC_ERR_INVALID_ARGUMENT,
+                        std::string("positive ") + names[k] + " count with null records");
+    }
+    recs.clear();
+    off.assign(N + 1, 0);
+    size_t pos[6] = {0, 0, 0, 0, 0, 0};
+    max_prims = 0;
+    for (int i = 0; i < N; ++i) {
+        for (int k = 0; k < 5; ++k) {
+            uint32_t c = cnt[k] ? cnt[k][i] : 0;
+            for (uint32_t j = 0; j < c; ++j) {
+                const float* r = rec[k] + (pos[k] + j) * width[k];
+                switch (k) {
+                    case 0: recs.push_back(rec_sphere(r)); break;
+                    case 1: recs.push_back(rec_capsule(r, false)); break;
+                    case 2: recs.push_back(rec_capsule(r, true)); break;
+                    case 3: recs.push_back(rec_cuboid(r, false)); break;
+                    case 4: recs.push_back(rec_cuboid(r, true)); break;
+                }
+            }
+            pos[k] += c;
+        }
+        if (cnt[5]) pos[5] += cnt[5][i];  // cylinders: never tested (src/utils.cuh:213-245)
+        off[i + 1] = (int)recs.size();
+        max_prims = std::max(max_prims, off[i + 1] - off[i]);
+        if (recs.size() > (size_t)0x7fffffff) return fail(ctx, BCC_ERR_LIMIT, "too many primitives");
+    }
+    if (max_prims > 4095) return fail(ctx, BCC_ERR_LIMIT, "more than 4095 primitives in one environment");
+    return BCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+bcc_status bcc_pack_envs(const bcc_env_soa* envs, float* records, int32_t* env_offsets, int64_t* num_records,
+                         int32_t* max_prims_per_env) {
+    std::vector<Rec> recs;
+    std::vector<int> off;
+    int max_prims = 0;
+    bcc_status s = pack(nullptr, envs, recs, off, max_prims);
+    if (s != BCC_OK) return s;
+    if (num_records) *num_records = (int64_t)recs.size();
+    if (max_prims_per_env) *max_prims_per_env = max_prims;
+    if (records && !recs.empty()) std::memcpy(records, recs.data(), recs.size() * sizeof(Rec));
+    if (env_offsets) std::memcpy(env_offsets, off.data(), off.size() * sizeof(int));
+    return BCC_OK;
+}
+
+bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    std::vector<Rec> recs;
+    std::vector<int> off;
+    int max_prims = 0;
+    bcc_status s = pack(ctx, envs, recs, off, max_prims);
+    if (s != BCC_OK) return s;
+    const int N = envs->num_envs;
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    BCC_CUDA(ctx, ctx->prims.ensure(std::max<size_t>(1, recs.size()) * sizeof(Rec)));
+    BCC_CUDA(ctx, ctx->env_off.ensure(sizeof(int) * (N + 1)));
+    if (!recs.empty())
+        BCC_CUDA(ctx, cudaMemcpy(ctx->prims.p, recs.data(), recs.size() * sizeof(Rec), cudaMemcpyHostToDevice));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->env_off.p, off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+    ctx->num_envs = N;
+    ctx->max_prims = max_prims;
+    return BCC_OK;
+}
+
+bcc_status bcc_check_device(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int32_t num_edges,
+                            int32_t resolution, uint8_t* d_results, const bcc_opts* opts, void* stream) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs < 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (num_edges < 0 || resolution <= 0) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad edge count or resolution");
+    if (num_edges == 0 || ctx->num_envs == 0) return BCC_OK;
+    if (!d_edges || !d_results) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "null edges or results");
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    return run_check(ctx, robot, d_edges, num_edges, resolution, d_results, opts,
+                     static_cast<cudaStream_t>(stream));
+}
+
+bcc_status bcc_check(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                     uint8_t* results, const bcc_opts* opts) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs < 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (num_edges < 0 || resolution <= 0) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad edge count or resolution");
+    const int dof = bcc_robot_dof(robot);
+    if (dof < 0) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "unknown robot");
+    if (num_edges == 0 || ctx->num_envs == 0) return BCC_OK;
+    if (!edges || !results) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "null edges or results");
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t eb = sizeof(float) * 2 * (size_t)dof * num_edges;
+    const size_t rb = (size_t)num_edges * ctx->num_envs;
+    BCC_CUDA(ctx, ctx->edges.ensure(eb));
+    BCC_CUDA(ctx, ctx->results.ensure(rb));
+    cudaStream_t st = ctx->stream;
+    BCC_CUDA(ctx, cudaMemcpyAsync(ctx->edges.p, edges, eb, cudaMemcpyHostToDevice, st));
+    bcc_status s = run_check(ctx, robot, ctx->edges.as<float>(), num_edges, resolution,
+                             ctx->results.as<uint8_t>(), opts, st);
+    if (s != BCC_OK) return s;
+    BCC_CUDA(ctx, cudaMemcpyAsync(results, ctx->results.p, rb, cudaMemcpyDeviceToHost, st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    int flag = 0;
+    BCC_CUDA(ctx, cudaMemcpy(&flag, ctx->error_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) return fail(ctx, BCC_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+    return BCC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// bcc_kernels.h -- host-visible launch interface of the checker kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bcc {
+
+struct CheckParams {
+    const float4* prims;     // [total prims][5] rounded-box records
+    const int* env_off;      // [num_envs + 1] first primitive of each env
+    int num_envs;
+    int max_prims;           // max primitives of one env (shared-memory sizing)
+    int envs_per_cta;
+    const int* steps;        // [E] n per edge
+    const int* offs;         // [E + 1] first sample row of each edge
+    const float4* table;     // [rows][num_spheres] sphere centres + radius
+    const float4* swept;     // [E][groups][2] cull AABB centre / half-size
+    const int* edge_self;    // [E] 1 when some sample self-collides
+    uint8_t* results;        // [E][num_envs]
+    int* error_flag;         // set when a bounded wait gives up
+};
+
+struct PipelineArgs {
+    const float* d_edges;    // [E][2][dof]
+    int num_edges;
+    int resolution;
+    int* steps;              // [E]
+    int* offs;               // [E + 1]
+    int total_rows;          // offs[E], read back after the scan
+    float4* table;           // [total_rows][num_spheres]
+    int* row_edge;           // [total_rows]
+    int* edge_self;          // [E]
+    float4* swept;           // [E][groups][2]
+    const float4* prims;
+    const int* env_off;
+    int num_envs;
+    int max_prims;
+    int envs_per_cta;
+    int warps;               // warps per check CTA (8, 4, 2 or 1)
+    uint8_t* d_results;
+    int* error_flag;
+    cudaEvent_t* stage_events;  // null, or 6 events bracketing the 5 stages
+};
+
+cudaError_t upload_robot_tables(int robot);
+// Stage 1: steps + sample offsets (total rows land in offs[E]).
+cudaError_t launch_steps(int robot, const PipelineArgs& a, cudaStream_t st);
+// Stage 2: FK table, self-collision, swept volumes, environment check.
+cudaError_t launch_check(int robot, const PipelineArgs& a, cudaStream_t st);
+size_t check_smem_bytes(int max_prims, int warps);
+int robot_num_spheres(int robot);
+int robot_num_env_groups(int robot);
+int robot_dof(int robot);
+
+}  // namespace bcc

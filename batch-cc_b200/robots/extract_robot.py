@@ -1,0 +1,323 @@
+"""Robot-model extractor: generated reference FK+CC code -> kinematic tables.
+
+The reference ships, per robot, one generated straight-line device function
+``fkcc<Robot>`` (``src/utils.cuh:342-5443`` for Panda).  It evaluates the
+forward kinematics of every collision sphere with scalar expressions and then
+runs a fixed hierarchy of tests:
+
+* environment checks (``src/utils.cuh:806-1190``): per link, a bounding
+  sphere gate followed by that link's leaf spheres; ``panda_link0`` is
+  commented out and never checked;
+* self checks (``src/utils.cuh:1192-5440``): per link pair, a bounding
+  sphere pair gate followed by the leaf-sphere pairs.
+
+This script reads that function as TEXT, evaluates its FK expressions in FP64
+with numpy, and re-expresses the robot as data of this project's own format:
+
+* a serial chain of revolute joints about local z (fixed transform per joint);
+* every sphere as (frame index, local offset, radius);
+* the gate/leaf structure of the environment and self checks, in the
+  reference's order.
+
+The chain parameters are the public Franka Panda joint origins; the script
+verifies that the chain reproduces every sphere centre of the generated code
+to FP64 rounding over random configurations before writing anything.
+
+Usage (reads the reference tree; run in the development container only)::
+
+    python extract_robot.py <path-to-reference>/src/utils.cuh panda panda.json
+"""
+import json
+import math
+import re
+import sys
+
+import numpy as np
+
+# cos/sin of the rounded right angle used by the robot description the
+# generated code was produced from (its FK carries cos(1.57079632679) =
+# 4.89663865010925e-12 wherever a joint frame is rotated by +-90 degrees).
+HALF_PI_DESC = 1.57079632679
+
+# Franka Panda joint origins (xyz, rpy) of joints 1..7; each joint rotates
+# about its local z axis.  Public robot description values.
+PANDA_JOINTS = [
+    ((0.0, 0.0, 0.333), (0.0, 0.0, 0.0)),
+    ((0.0, 0.0, 0.0), (-HALF_PI_DESC, 0.0, 0.0)),
+    ((0.0, -0.316, 0.0), (HALF_PI_DESC, 0.0, 0.0)),
+    ((0.0825, 0.0, 0.0), (HALF_PI_DESC, 0.0, 0.0)),
+    ((-0.0825, 0.384, 0.0), (-HALF_PI_DESC, 0.0, 0.0)),
+    ((0.0, 0.0, 0.0), (HALF_PI_DESC, 0.0, 0.0)),
+    ((0.088, 0.0, 0.0), (HALF_PI_DESC, 0.0, 0.0)),
+]
+
+# link name -> chain frame the link is rigidly attached to (0 = base).
+PANDA_LINK_FRAME = {
+    "panda_link0": 0, "panda_link1": 1, "panda_link2": 2, "panda_link3": 3,
+    "panda_link4": 4, "panda_link5": 5, "panda_link6": 6, "panda_link7": 7,
+    "panda_hand": 7, "panda_leftfinger": 7, "panda_rightfinger": 7,
+}
+
+
+def rpy_matrix(r, p, y):
+    cr, sr = math.cos(r), math.sin(r)
+    cp, sp = math.cos(p), math.sin(p)
+    cy, sy = math.cos(y), math.sin(y)
+    rx = np.array([[1, 0, 0], [0, cr, -sr], [0, sr, cr]])
+    ry = np.array([[cp, 0, sp], [0, 1, 0], [-sp, 0, cp]])
+    rz = np.array([[cy, -sy, 0], [sy, cy, 0], [0, 0, 1]])
+    return rz @ ry @ rx
+
+
+def fixed_tf(xyz, rpy):
+    t = np.eye(4)
+    t[:3, :3] = rpy_matrix(*rpy)
+    t[:3, 3] = xyz
+    return t
+
+
+def rot_z(q):
+    c, s = math.cos(q), math.sin(q)
+    t = np.eye(4)
+    t[0, 0], t[0, 1], t[1, 0], t[1, 1] = c, -s, s, c
+    return t
+
+
+def chain_frames(joints, q):
+    """World transforms of frames 0..len(joints) for configuration q (FP64)."""
+    frames = [np.eye(4)]
+    for (xyz, rpy), qj in zip(joints, q):
+        frames.append(frames[-1] @ fixed_tf(xyz, rpy) @ rot_z(qj))
+    return frames
+
+
+def _function_body(text, robot_struct):
+    m = re.search(r"fkcc<ppln::robots::%s>\(volatile float \*(\w+)" % robot_struct, text)
+    if not m:
+        raise SystemExit("fkcc<%s> not found" % robot_struct)
+    start = text.index("{", m.end())
+    depth, i = 0, start
+    while True:
+        c = text[i]
+        if c == "{":
+            depth += 1
+        elif c == "}":
+            depth -= 1
+            if depth == 0:
+                return m.group(1), text[start + 1:i]
+        i += 1
+
+
+def _strip_line_comment(line):
+    k = line.find("//")
+    return line if k < 0 else line[:k]
+
+
+def parse_panda_style(body):
+    """Split a Panda-style generated body into FK statements and checks."""
+    lines = body.split("\n")
+    # FK: everything before the first environment check.
+    first_if = next(i for i, l in enumerate(lines) if "sphere_environment_in_collision" in l)
+    fk_text = "\n".join(_strip_line_comment(l) for l in lines[:first_if])
+    fk_text = fk_text.rsplit("if", 1)[0] if fk_text.rstrip().endswith("(") else fk_text
+    stmts = []
+    for s in fk_text.split(";"):
+        s = " ".join(s.split())
+        if not s:
+            continue
+        s = re.sub(r"^float\s+", "", s)
+        name, expr = s.split("=", 1)
+        stmts.append((name.strip(), expr.strip()))
+
+    # Checks: walk lines after the FK, track brace depth and link comments.
+    env_groups, self_groups = [], []
+    depth = 0
+    cur_link = None
+    pending = None  # accumulates a multi-line call
+    call_re_env = re.compile(r"sphere_environment_in_collision\(\s*environment\s*,([^)]*)\)")
+    call_re_self = re.compile(r"sphere_sphere_self_collision\(([^)]*)\)")
+    for raw in lines[first_if - 3:]:
+        cm = re.match(r"\s*//\s*(panda_\w+)(?:\s+vs\.\s+(panda_\w+))?\s*$", raw)
+        if cm:
+            cur_link = (cm.group(1), cm.group(2))
+            continue
+        line = _strip_line_comment(raw)
+        if pending is not None:
+            pending += " " + line
+        elif "sphere_environment_in_collision" in line or "sphere_sphere_self_collision" in line:
+            pending = line
+        if pending is not None and pending.count("(") <= pending.count(")"):
+            me = call_re_env.search(pending)
+            ms = call_re_self.search(pending)
+            if me:
+                args = [a.strip() for a in me.group(1).split(",")]
+                if depth == 0:
+                    env_groups.append({"link": cur_link[0], "bound": args, "leaves": []})
+                else:
+                    env_groups[-1]["leaves"].append(args)
+            elif ms:
+                args = [a.strip() for a in ms.group(1).split(",")]
+                a, b = args[:4], args[4:]
+                if depth == 0:
+                    self_groups.append({"links": list(cur_link), "bound": [a, b], "leaves": []})
+                else:
+                    self_groups[-1]["leaves"].append([a, b])
+            pending = None
+        depth += line.count("{") - line.count("}")
+    return stmts, env_groups, self_groups
+
+
+def make_evaluator(stmts, qname):
+    code = []
+    for name, expr in stmts:
+        e = expr.replace("__sinf(", "np.sin(").replace("__cosf(", "np.cos(")
+        e = re.sub(r"%s\[(\d+)\]" % qname, r"q[\1]", e)
+        code.append("    %s = %s" % (name, e))
+    names = sorted({n for n, _ in stmts})
+    src = "def fk(q):\n" + "\n".join(code) + "\n    return {%s}\n" % ", ".join(
+        "'%s': %s" % (n, n) for n in names)
+    ns = {"np": np}
+    exec(src, ns)  # the expressions are plain arithmetic on q
+    return ns["fk"]
+
+
+def extract_panda(utils_path):
+    text = open(utils_path).read()
+    qname, body = _function_body(text, "Panda")
+    stmts, env_groups, self_groups = parse_panda_style(body)
+    fk = make_evaluator(stmts, qname)
+    dof = 7
+
+    # Collect every sphere referenced by a check: (x, y, z, r) variable tuples.
+    sphere_keys = []
+    def key_of(args):
+        k = tuple(args)
+        if k not in sphere_keys:
+            sphere_keys.append(k)
+        return sphere_keys.index(k)
+
+    link_of = {}
+    envs = []
+    for g in env_groups:
+        b = key_of(g["bound"])
+        link_of[b] = g["link"]
+        leaves = []
+        for l in g["leaves"]:
+            i = key_of(l)
+            link_of[i] = g["link"]
+            leaves.append(i)
+        envs.append({"link": g["link"], "bound": b, "leaves": leaves})
+    selfs = []
+    for g in self_groups:
+        la, lb = g["links"]
+        ba, bb = key_of(g["bound"][0]), key_of(g["bound"][1])
+        link_of.setdefault(ba, la)
+        link_of.setdefault(bb, lb)
+        pairs = []
+        for a, b in g["leaves"]:
+            ia, ib = key_of(a), key_of(b)
+            link_of.setdefault(ia, la)
+            link_of.setdefault(ib, lb)
+            pairs.append([ia, ib])
+        selfs.append({"links": [la, lb], "bound": [ba, bb], "pairs": pairs})
+
+    rng = np.random.default_rng(1234)
+    def value(vals, tok):
+        try:
+            return float(tok)
+        except ValueError:
+            return float(vals[tok])
+
+    # Local offsets from q = random reference pose, then verification.
+    q0 = rng.uniform(-3.0, 3.0, dof)
+    vals = fk(q0)
+    frames = chain_frames(PANDA_JOINTS, q0)
+    spheres = []
+    for idx, k in enumerate(sphere_keys):
+        frame = PANDA_LINK_FRAME[link_of[idx]]
+        p = np.array([value(vals, t) for t in k[:3]] + [1.0])
+        local = np.linalg.solve(frames[frame], p)[:3]
+        r = float(np.float32(value(vals, k[3])))
+        spheres.append({"frame": frame, "local": local.tolist(), "r": r,
+                        "link": link_of[idx], "src": list(k)})
+
+    max_err = 0.0
+    for _ in range(2000):
+        q = rng.uniform(-4.0, 4.0, dof)
+        vals = fk(q)
+        frames = chain_frames(PANDA_JOINTS, q)
+        for s in spheres:
+            p = frames[s["frame"]] @ np.array(s["local"] + [1.0])
+            ref = np.array([value(vals, t) for t in s["src"][:3]])
+            max_err = max(max_err, float(np.abs(p[:3] - ref).max()))
+    if max_err > 1e-12:
+        raise SystemExit("chain does not reproduce the generated FK: max err %g" % max_err)
+
+    # Leaf-in-bound containment (decides whether gates can change verdicts).
+    contain = []
+    for g in envs:
+        b = spheres[g["bound"]]
+        worst = -1e9
+        for i in g["leaves"]:
+            s = spheres[i]
+            assert s["frame"] == b["frame"]
+            d = np.linalg.norm(np.array(s["local"]) - np.array(b["local"])) + s["r"] - b["r"]
+            worst = max(worst, d)
+        contain.append({"link": g["link"], "leaf_excess_m": worst})
+    for g in selfs:
+        for side in (0, 1):
+            b = spheres[g["bound"][side]]
+            worst = -1e9
+            for p in g["pairs"]:
+                s = spheres[p[side]]
+                d = np.linalg.norm(np.array(s["local"]) - np.array(b["local"])) + s["r"] - b["r"]
+                worst = max(worst, d)
+            contain.append({"link": g["links"][side], "pair": g["links"], "leaf_excess_m": worst})
+
+    return {
+        "robot": "panda",
+        "dof": dof,
+        "joints": [{"xyz": list(x), "rpy": list(r)} for x, r in PANDA_JOINTS],
+        "spheres": [{k: s[k] for k in ("frame", "local", "r", "link")} for s in spheres],
+        "env_groups": envs,
+        "self_groups": selfs,
+        "containment": contain,
+        "fk_max_abs_err_vs_generated_code_m": max_err,
+        "_fk_eval": fk,
+        "_sphere_src": [s["src"] for s in spheres],
+    }
+
+
+def main():
+    utils_path, robot, out = sys.argv[1], sys.argv[2], sys.argv[3]
+    if robot != "panda":
+        raise SystemExit("only panda is extracted by this script version")
+    model = extract_panda(utils_path)
+    fk = model.pop("_fk_eval")
+    src = model.pop("_sphere_src")
+    # Golden FK vectors: sphere centres of the generated code (FP64) at seeded q.
+    rng = np.random.default_rng(20261203)
+    gold = []
+    for _ in range(64):
+        q = rng.uniform(-3.2, 3.9, model["dof"]).astype(np.float32).astype(np.float64)
+        vals = fk(q)
+        cs = []
+        for k in src:
+            cs.append([float(vals[t]) if not re.match(r"^-?[\d.]", t) else float(t) for t in k[:3]])
+        gold.append({"q": q.tolist(), "centres": cs})
+    with open(out, "w") as f:
+        json.dump(model, f, indent=1)
+    if len(sys.argv) > 4:
+        with open(sys.argv[4], "w") as f:
+            json.dump({"robot": robot, "cases": gold}, f)
+    print("spheres=%d env_groups=%d self_groups=%d self_pairs=%d fk_err=%.3g" % (
+        len(model["spheres"]), len(model["env_groups"]), len(model["self_groups"]),
+        sum(len(g["pairs"]) for g in model["self_groups"]),
+        model["fk_max_abs_err_vs_generated_code_m"]))
+    for c in model["containment"]:
+        if c["leaf_excess_m"] > 0:
+            print("leaf outside bound:", c)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,126 @@
+"""Write the C++/CUDA robot-model header from an extracted robot JSON.
+
+The header holds plain constexpr tables (joint fixed transforms, sphere
+frames/offsets/radii, environment and self check groups, joint-limit scale)
+inside one struct per robot, usable from host C++ (the CPU oracle) and from
+CUDA device code (the checker kernels), where unrolled loops over the tables
+fold every offset into immediate operands.
+
+Usage::
+
+    python gen_header.py panda.json ../csrc/robot_panda.h
+"""
+import json
+import math
+import sys
+
+import numpy as np
+
+# Joint-limit scale q = u * s_m + s_a, as the reference robot structs define
+# it (src/Robots.hh:17-41 Panda, :72-98 Fetch, :128-166 Baxter).
+LIMITS = {
+    "panda": ([5.9342, 3.6652, 5.9342, 3.2289, 5.9342, 3.9095999999999997, 5.9342],
+              [-2.9671, -1.8326, -2.9671, -3.1416, -2.9671, -0.0873, -2.9671]),
+}
+
+
+def rpy_matrix(r, p, y):
+    cr, sr = math.cos(r), math.sin(r)
+    cp, sp = math.cos(p), math.sin(p)
+    cy, sy = math.cos(y), math.sin(y)
+    rx = np.array([[1, 0, 0], [0, cr, -sr], [0, sr, cr]])
+    ry = np.array([[cp, 0, sp], [0, 1, 0], [-sp, 0, cp]])
+    rz = np.array([[cy, -sy, 0], [sy, cy, 0], [0, 0, 1]])
+    return rz @ ry @ rx
+
+
+def fmt(v):
+    return repr(float(v))
+
+
+def main():
+    src, out = sys.argv[1], sys.argv[2]
+    m = json.load(open(src))
+    name = m["robot"]
+    S = name.capitalize() + "Model"
+    dof = m["dof"]
+    sph = m["spheres"]
+    env = m["env_groups"]
+    slf = m["self_groups"]
+    s_m, s_a = LIMITS[name]
+
+    lines = []
+    w = lines.append
+    w("// Generated by batch-cc_b200/robots/gen_header.py from %s.json -- do not edit." % name)
+    w("// Kinematic chain + collision-sphere tables of the %s robot, extracted from the" % name)
+    w("// reference's generated fkcc<%s> (src/utils.cuh) and verified against it in FP64." % name.capitalize())
+    w("#pragma once")
+    w("")
+    w("namespace bcc {")
+    w("")
+    w("struct %s {" % S)
+    w("    static constexpr int dof = %d;" % dof)
+    w("    static constexpr int num_spheres = %d;" % len(sph))
+    w("    static constexpr int num_env_groups = %d;" % len(env))
+    w("    static constexpr int num_env_leaves = %d;" % sum(len(g["leaves"]) for g in env))
+    w("    static constexpr int num_self_groups = %d;" % len(slf))
+    w("    static constexpr int num_self_pairs = %d;" % sum(len(g["pairs"]) for g in slf))
+    w("")
+    w("    // Fixed transform of joint k (row-major 3x4: rotation | translation); the joint")
+    w("    // then rotates about its local z axis.  frame k+1 = frame k * F_k * Rz(q_k).")
+    w("    static constexpr double joint_tf[%d][12] = {" % dof)
+    for j in m["joints"]:
+        R = rpy_matrix(*j["rpy"])
+        t = j["xyz"]
+        vals = [R[0, 0], R[0, 1], R[0, 2], t[0], R[1, 0], R[1, 1], R[1, 2], t[1],
+                R[2, 0], R[2, 1], R[2, 2], t[2]]
+        w("        {%s}," % ", ".join(fmt(v) for v in vals))
+    w("    };")
+    w("")
+    w("    // Sphere k: chain frame (0 = base), offset in that frame (m), radius (m, float).")
+    w("    static constexpr int sphere_frame[%d] = {%s};" % (
+        len(sph), ", ".join(str(s["frame"]) for s in sph)))
+    w("    static constexpr double sphere_local[%d][3] = {" % len(sph))
+    for s in sph:
+        w("        {%s}," % ", ".join(fmt(v) for v in s["local"]))
+    w("    };")
+    w("    static constexpr float sphere_radius[%d] = {%s};" % (
+        len(sph), ", ".join(repr(float(np.float32(s["r"]))) + "f" for s in sph)))
+    w("")
+    w("    // Environment checks in reference order: group g gates on sphere env_bound[g]")
+    w("    // and then tests leaves env_leaves[env_leaf_begin[g] .. env_leaf_begin[g+1]).")
+    w("    static constexpr int env_bound[%d] = {%s};" % (len(env), ", ".join(str(g["bound"]) for g in env)))
+    begins = [0]
+    for g in env:
+        begins.append(begins[-1] + len(g["leaves"]))
+    w("    static constexpr int env_leaf_begin[%d] = {%s};" % (len(begins), ", ".join(map(str, begins))))
+    w("    static constexpr int env_leaves[%d] = {%s};" % (
+        begins[-1], ", ".join(str(i) for g in env for i in g["leaves"])))
+    w("")
+    w("    // Self checks in reference order: group g gates on the bound pair self_bound[g]")
+    w("    // and then tests the leaf pairs self_pairs[self_pair_begin[g] .. self_pair_begin[g+1]).")
+    w("    static constexpr int self_bound[%d][2] = {%s};" % (
+        len(slf), ", ".join("{%d, %d}" % tuple(g["bound"]) for g in slf)))
+    pb = [0]
+    for g in slf:
+        pb.append(pb[-1] + len(g["pairs"]))
+    w("    static constexpr int self_pair_begin[%d] = {%s};" % (len(pb), ", ".join(map(str, pb))))
+    w("    static constexpr unsigned char self_pairs[%d][2] = {" % pb[-1])
+    flat = ["{%d, %d}" % tuple(p) for g in slf for p in g["pairs"]]
+    for i in range(0, len(flat), 12):
+        w("        %s," % ", ".join(flat[i:i + 12]))
+    w("    };")
+    w("")
+    w("    // Joint-limit scale of the robot description: q = u * s_m + s_a.")
+    w("    static constexpr float s_m[%d] = {%s};" % (dof, ", ".join(repr(float(np.float32(v))) + "f" for v in s_m)))
+    w("    static constexpr float s_a[%d] = {%s};" % (dof, ", ".join(repr(float(np.float32(v))) + "f" for v in s_a)))
+    w("};")
+    w("")
+    w("}  // namespace bcc")
+    w("")
+    open(out, "w").write("\n".join(lines))
+    print("wrote", out)
+
+
+if __name__ == "__main__":
+    main()

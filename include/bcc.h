@@ -1,0 +1,160 @@
+/*
+ * bcc.h -- C ABI of the B200 batch edge collision checker.
+ *
+ * Drop-in boundary for the reference entry point
+ *   template <typename Robot> void batch_cc::batch_cc(
+ *       std::vector<ppln::collision::Environment<float>>& h_envs,
+ *       std::vector<std::array<typename Robot::Configuration, 2>>& edges,
+ *       int resolution, std::vector<bool>& results);
+ * declared at src/batch_cc.hh:4-6 and defined at src/batch_cc.cu:244-338.
+ *
+ * Every entry point takes plain pointers and sizes (no C++ or torch types) and
+ * returns a bcc_status.  Verdicts keep the reference's meaning and layout:
+ * results[edge * num_envs + env] = 1 when the discretised edge is IN COLLISION
+ * in that environment (src/batch_cc.cu:130-132), 0 when it is free.
+ */
+#ifndef BCC_H
+#define BCC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bcc_status {
+    BCC_OK = 0,
+    BCC_ERR_INVALID_ARGUMENT = 1, /* null pointer with a positive count, bad size, unknown robot */
+    BCC_ERR_CUDA = 2,             /* a CUDA runtime call failed; see bcc_last_error */
+    BCC_ERR_NO_ENVS = 3,          /* bcc_check before any bcc_upload_envs */
+    BCC_ERR_TIMEOUT = 4,          /* a bounded device-side wait gave up */
+    BCC_ERR_NOT_SUPPORTED = 5,    /* option or robot not available in this build */
+    BCC_ERR_LIMIT = 6             /* a size exceeds a documented maximum */
+} bcc_status;
+
+typedef enum bcc_robot {
+    BCC_ROBOT_PANDA = 0,  /* src/Robots.hh:10-64, 7 DOF */
+    BCC_ROBOT_FETCH = 1,  /* src/Robots.hh:66-120, 8 DOF */
+    BCC_ROBOT_BAXTER = 2  /* src/Robots.hh:122-188, 14 DOF */
+} bcc_robot;
+
+/*
+ * Environments in structure-of-arrays form: per-environment primitive counts,
+ * and the records of all environments concatenated in environment order.
+ * Record layouts follow the reference shapes (src/collision/shapes.hh) without
+ * their std::string header:
+ *   sphere   [4]  x y z r                                   (shapes.hh:226-245)
+ *   capsule  [8]  x1 y1 z1 xv yv zv r rdv  (rdv = 1/|v|^2)  (shapes.hh:131-222)
+ *   cuboid   [15] x y z  a1x a1y a1z  a2x a2y a2z  a3x a3y a3z  h1 h2 h3
+ *                                                           (shapes.hh:30-126)
+ * z_capsules / z_cuboids are the axis-aligned variants tested with the
+ * reference's z-aligned predicates (src/utils.cuh:138-156, :187-210).
+ * Cylinders are accepted but, exactly as in the reference device scan
+ * (src/utils.cuh:213-245), never tested: the reference drivers pass
+ * cylinders as capsules.
+ * A null count array means zero primitives of that kind in every environment.
+ */
+typedef struct bcc_env_soa {
+    int32_t num_envs;
+    const uint32_t* num_spheres;
+    const uint32_t* num_capsules;
+    const uint32_t* num_z_capsules;
+    const uint32_t* num_cuboids;
+    const uint32_t* num_z_cuboids;
+    const uint32_t* num_cylinders;
+    const float* spheres;
+    const float* capsules;
+    const float* z_capsules;
+    const float* cuboids;
+    const float* z_cuboids;
+    const float* cylinders;
+} bcc_env_soa;
+
+/* Sample-check order inside each (environment, edge) pair. */
+typedef enum bcc_order {
+    BCC_ORDER_PLAIN = 0,   /* ascending sample index */
+    BCC_ORDER_LEARNED = 1  /* descending collision likelihood from the proposal MLP */
+} bcc_order;
+
+typedef struct bcc_opts {
+    int32_t order;         /* bcc_order */
+    int32_t use_graph;     /* 1: replay a captured CUDA graph of the launch sequence */
+    int32_t tile_override; /* 0: autotuned tile; >0: force a tile id (tuning/tests) */
+    int32_t reserved;
+} bcc_opts;
+
+typedef struct bcc_ctx bcc_ctx;
+
+/* Context lifetime.  A context owns device buffers that persist across calls. */
+bcc_status bcc_create(bcc_ctx** out, int device);
+void bcc_destroy(bcc_ctx* ctx);
+const char* bcc_last_error(const bcc_ctx* ctx);
+
+/*
+ * Upload (replace) the environment set.  Replaces the reference's per-env
+ * setup_environment_on_device / cleanup_environment_on_device
+ * (src/batch_cc.cu:135-240) with one packed device arena.  Rejects a positive
+ * count with a null record pointer, like ensure_ptr_count_consistent
+ * (src/batch_cc.cu:45-56).
+ */
+bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs);
+
+/*
+ * Check every (environment, edge) pair.  edges: host array float[num_edges][2][dof]
+ * (start, end), the reference's layout (src/batch_cc.cu:292-295).  results: host
+ * array of num_envs * num_edges bytes, edge-major.  resolution: the reference's
+ * step multiplier (32 in its drivers, scripts/batch_cc_mbm.cpp:184).
+ * Synchronous: returns after the verdicts are in host memory.
+ */
+bcc_status bcc_check(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges,
+                     int32_t resolution, uint8_t* results, const bcc_opts* opts);
+
+/*
+ * Device-resident variant: edges and results are device pointers; the call is
+ * stream-ordered on `stream` (a cudaStream_t, 0 = legacy default stream) and
+ * returns without synchronising.
+ */
+bcc_status bcc_check_device(bcc_ctx* ctx, bcc_robot robot, const float* d_edges,
+                            int32_t num_edges, int32_t resolution, uint8_t* d_results,
+                            const bcc_opts* opts, void* stream);
+
+/*
+ * Host-only helper (no CUDA call): pack an environment set into the device
+ * arena format -- one 80-byte "rounded box" record per primitive (20 floats:
+ * centre xyz, rounding radius; axis1 xyz, h1; axis2 xyz, h2; axis3 xyz, h3;
+ * cull AABB half-size xyz, 0) and env_offsets[num_envs + 1] (first record of
+ * each environment).  Pass records = NULL to query the record count through
+ * *num_records.  Performs the same validation as bcc_upload_envs.
+ */
+bcc_status bcc_pack_envs(const bcc_env_soa* envs, float* records, int32_t* env_offsets,
+                         int64_t* num_records, int32_t* max_prims_per_env);
+
+/*
+ * Stage timing.  With profiling on, every check records CUDA events around its
+ * stages on the launch stream; bcc_stage_times returns the last check's device
+ * milliseconds (after the stream has been synchronised by the caller):
+ *   [0] discretisation + sample offsets  [1] forward kinematics table
+ *   [2] self-collision                    [3] swept cull volumes
+ *   [4] environment check (the dominant kernel)
+ * Returns the number of stages written, or -1.
+ */
+bcc_status bcc_set_profiling(bcc_ctx* ctx, int32_t on);
+int32_t bcc_stage_times(bcc_ctx* ctx, float* ms, int32_t max_stages);
+
+/* Diagnostics: FP32 FMA-pipe throughput of `device` in TFLOP/s, measured by a
+ * short probe kernel (the roofline denominator of the scalar-FP32 checker). */
+bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
+
+/* Number of samples the reference discretisation checks for one edge
+ * (32 * max(ceil(|end - start|_2 / 31 * resolution), 1), src/batch_cc.cu:103-116). */
+int32_t bcc_edge_samples(const float* start, const float* end, int32_t dof, int32_t resolution);
+
+/* Robot degrees of freedom (7, 8, 14), or -1 for an unknown robot. */
+int32_t bcc_robot_dof(bcc_robot robot);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BCC_H */

@@ -1,0 +1,198 @@
+"""CPU tests of the oracle: pinned to the reference's generated FK, the
+reference discretisation rules, and hand-built known-answer cases."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from bcc import EnvSet, workload
+from bcc.workload import make_capsules, make_cuboids, make_spheres
+from oracle import oracle as orc
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_fk_matches_reference_generated_code():
+    """Sphere centres of the chain tables == the reference's generated fkcc<Panda>
+    FK expressions evaluated in FP64 (tests/golden/panda_fk_generated.json)."""
+    g = json.load(open(os.path.join(GOLDEN, "panda_fk_generated.json")))
+    assert len(g["cases"]) >= 32
+    worst = 0.0
+    for c in g["cases"]:
+        q = np.array(c["q"], np.float32)
+        assert np.array_equal(q.astype(np.float64), np.array(c["q"]))
+        got = orc.fk(q)
+        want = np.array(c["centres"])
+        worst = max(worst, float(np.abs(got - want).max()))
+    assert worst < 1e-12, worst
+
+
+def test_discretisation_rules():
+    # n = max(ceil(|e - s| / 31 * 32), 1): a zero-length edge still checks 32 samples.
+    s = np.zeros(7, np.float32)
+    assert orc.edge_n(s, s) == 1
+    assert len(orc.edge_samples(s, s)) == 32
+    e = s.copy()
+    e[0] = 31.0 / 32.0  # exactly one step boundary
+    assert orc.edge_n(s, e) == 1
+    e[0] = np.nextafter(np.float32(31.0 / 32.0), np.float32(2))
+    assert orc.edge_n(s, e) == 2
+    e[0] = 12.0
+    assert orc.edge_n(s, e) == int(np.ceil(12.0 / 31.0 * 32.0))
+
+
+def test_sample_set_overshoots_like_reference():
+    """Samples t_k = k / (31 n), k < 32 n: lane 31's first sample is the goal and
+    the last sample lies past it (src/batch_cc.cu:109-129)."""
+    rng = np.random.default_rng(0)
+    for _ in range(50):
+        s = rng.uniform(-2, 2, 7).astype(np.float32)
+        e = (s + rng.uniform(-1.5, 1.5, 7)).astype(np.float32)
+        n = orc.edge_n(s, e)
+        S = orc.edge_samples(s, e)
+        assert S.shape == (32 * n, 7)
+        assert np.array_equal(S[0], s)  # k = 0 is the start, exactly
+        t = np.arange(32 * n) / (31.0 * n)
+        ideal = s[None, :].astype(np.float64) + t[:, None] * (e - s)[None, :].astype(np.float64)
+        assert np.abs(S - ideal).max() < 1e-5
+        assert np.abs(S[31 * n] - e).max() < 1e-5  # lane 31 starts at the goal
+
+
+def test_bcc_edge_samples_matches_oracle():
+    from bcc import lib as bcclib
+
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        s = rng.uniform(-3, 3, 7).astype(np.float32)
+        e = rng.uniform(-3, 3, 7).astype(np.float32)
+        assert bcclib.edge_samples(s, e) == 32 * orc.edge_n(s, e)
+
+
+def _pose_with_hand_sphere():
+    q = np.array([0.3, -0.4, 0.2, -2.0, 0.1, 1.8, 0.5], np.float32)
+    c = orc.fk(q)
+    return q, c
+
+
+def _tip_and_approach(c):
+    """Outermost right-finger leaf (sphere 2) and the hand's approach axis
+    (frame-7 z, through spheres 26 and 6): obstacles placed beyond the tip
+    along it are nearest to that leaf alone."""
+    d = c[6] - c[26]
+    return 2, d / np.linalg.norm(d)
+
+
+def test_known_answer_touching_sphere():
+    """One obstacle sphere 1e-4 m outside / inside contact with the fingertip
+    sphere (radius + 0.005 inflation): free / collision."""
+    q, c = _pose_with_hand_sphere()
+    tip, d = _tip_and_approach(c)
+    r_tip = 0.012000000104308128
+    r_obs = 0.05
+    for gap, want in ((1e-4, 0), (-1e-4, 1)):
+        centre = c[tip] + d * (r_tip + 0.005 + r_obs + gap)
+        envs = EnvSet.from_lists([{"spheres": make_spheres(centre[None, :], np.array([r_obs]))}])
+        edge = np.stack([q, q])[None]
+        v = orc.check(envs, edge)
+        pen, _ = orc.pair_pen(envs, edge, [[0, 0]])
+        assert v[0, 0] == want, (gap, pen)
+        assert abs(pen[0] + gap) < 2e-6
+
+
+def test_empty_env_only_self_collision():
+    edges = workload.gen_edges("uneven", 200, seed=5)
+    empty = EnvSet.from_lists([{}, {}])
+    v = orc.check(empty, edges)
+    assert np.array_equal(v[:, 0], v[:, 1])
+    assert 0 < v[:, 0].mean() < 0.5  # some edges self-collide, most do not
+
+
+def test_zero_length_capsule_is_sphere():
+    rng = np.random.default_rng(3)
+    cen = rng.uniform(-0.5, 0.5, (6, 3))
+    cap = make_capsules(cen, np.zeros((6, 3)), np.full(6, 0.08), np.zeros(6))
+    assert np.all(np.isinf(cap[:, 7]))
+    sph = make_spheres(cen, np.full(6, 0.08))
+    envs = EnvSet.from_lists([{"capsules": cap}, {"spheres": sph}])
+    edges = workload.gen_edges("plain", 60, seed=3)
+    v = orc.check(envs, edges)
+    assert np.array_equal(v[:, 0], v[:, 1])
+
+
+def test_cylinders_are_never_tested():
+    rng = np.random.default_rng(4)
+    cyl = make_capsules(rng.uniform(-0.2, 0.2, (4, 3)), np.zeros((4, 3)), np.full(4, 0.3), np.full(4, 1.0))
+    envs = EnvSet.from_lists([{"cylinders": cyl}, {}])
+    edges = workload.gen_edges("plain", 40, seed=4)
+    v = orc.check(envs, edges)
+    assert np.array_equal(v[:, 0], v[:, 1])
+
+
+def test_fp32_and_fp64_oracles_agree_up_to_contact():
+    envs = workload.gen_envs("uneven", 24, seed=11)
+    edges = workload.gen_edges("uneven", 120, seed=11)
+    v64 = orc.check(envs, edges, precision=64)
+    v32 = orc.check(envs, edges, precision=32)
+    n, adj, bad = orc.adjudicate(envs, edges, v32, v64)
+    assert len(bad) == 0
+
+
+def test_penetration_sign_matches_verdict():
+    envs = workload.gen_envs("plain", 6, seed=2)
+    edges = workload.gen_edges("plain", 40, seed=2)
+    v = orc.check(envs, edges)
+    pairs = np.array([(e, i) for e in range(40) for i in range(6)])
+    pen, _ = orc.pair_pen(envs, edges, pairs)
+    verdict = v[pairs[:, 0], pairs[:, 1]]
+    assert np.all(pen[verdict == 1] > -1e-9)
+    assert np.all(pen[verdict == 0] < 1e-9)
+
+
+def test_known_answer_rotated_cuboid_face():
+    """A rotated cuboid whose face lies 1e-4 m outside / inside the inflated
+    fingertip sphere: free / collision."""
+    q, c = _pose_with_hand_sphere()
+    tip, d = _tip_and_approach(c)
+    r_inf = 0.012000000104308128 + 0.005
+    u = np.cross(d, [0.3, 0.5, 0.8])
+    u /= np.linalg.norm(u)
+    w = np.cross(d, u)
+    h = np.array([0.04, 0.05, 0.03])
+    for gap, want in ((1e-4, 0), (-1e-4, 1)):
+        centre = c[tip] + d * (r_inf + gap + h[0])
+        rec = np.zeros((1, 15), np.float32)
+        rec[0, 0:3] = centre
+        rec[0, 3:6], rec[0, 6:9], rec[0, 9:12] = d, u, w
+        rec[0, 12:15] = h
+        envs = EnvSet.from_lists([{"cuboids": rec}])
+        edge = np.stack([q, q])[None]
+        assert orc.check(envs, edge)[0, 0] == want
+
+
+LEAVES = [1, 2, 4, 5] + list(range(7, 25)) + list(range(26, 31)) + [32, 33, 34] + list(range(36, 48)) + \
+    [49, 50, 51, 52, 54, 55, 56, 57, 59, 60, 61, 62, 64, 65, 66, 67]
+
+
+def orc_radii():
+    m = json.load(open(os.path.join(os.path.dirname(__file__), "..", "batch-cc_b200", "robots", "panda.json")))
+    return np.array([s["r"] for s in m["spheres"]])
+
+
+def test_leaf_list_matches_model():
+    m = json.load(open(os.path.join(os.path.dirname(__file__), "..", "batch-cc_b200", "robots", "panda.json")))
+    leaves = sorted(i for g in m["env_groups"] for i in g["leaves"])
+    assert leaves == sorted(LEAVES)
+
+
+@pytest.mark.parametrize("name", ["plain", "uneven", "stress"])
+def test_workload_generators_are_seeded(name):
+    a = workload.gen_envs(name, 5, seed=9)
+    b = workload.gen_envs(name, 5, seed=9)
+    for k in a.records:
+        assert np.array_equal(a.records[k], b.records[k])
+    e1 = workload.gen_edges(name, 50, seed=9)
+    e2 = workload.gen_edges(name, 50, seed=9)
+    assert np.array_equal(e1, e2)
+    s_m, s_a = workload.LIMITS["panda"]
+    assert np.all(e1 >= s_a - 1e-5) and np.all(e1 <= s_a + s_m + 1e-5)
