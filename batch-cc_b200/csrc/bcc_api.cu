@@ -201,7 +201,9 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.offs + E, sizeof(int), cudaMemcpyDeviceToHost, st));
     BCC_CUDA(ctx, cudaStreamSynchronize(st));
     const int total = *ctx->h_total;
-    if (total < 0) return fail(ctx, BCC_ERR_LIMIT, "sample count overflows int32");
+    // offs[] is int32: the scan wraps past 2^31; cap the sample table at 2^27 rows.
+    if (total < 0 || total > (1 << 27))
+        return fail(ctx, BCC_ERR_LIMIT, "too many samples in one call (edges too long or non-finite)");
     const int NS = bcc::robot_num_spheres(r);
     BCC_CUDA(ctx, ctx->table.ensure(sizeof(float4) * (size_t)NS * std::max(total, 1)));
     BCC_CUDA(ctx, ctx->row_edge.ensure(sizeof(int) * (size_t)std::max(total, 1)));

@@ -83,7 +83,10 @@ __global__ void edge_steps_kernel(const float* __restrict__ edges, int E, int re
         s[j] = edges[(size_t)e * 2 * M::dof + j];
         t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
     }
-    steps[e] = edge_steps<M::dof>(s, t, resolution);
+    // Non-finite endpoints would give an unbounded step count: clamp, and let the
+    // host reject the resulting sample total (BCC_ERR_LIMIT).
+    const int n = edge_steps<M::dof>(s, t, resolution);
+    steps[e] = (n < 1 || n > (1 << 20)) ? (1 << 20) : n;
 }
 
 // ------------------------------------------------------------------ 2. scan
@@ -301,7 +304,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
         __syncwarp();
         if (nv < tile1) issue(nv, buf ^ 1);
         if (pending[buf]) {
-            if (!mbar_wait_bounded(&bars[warp][buf], phase[buf], 1u << 24)) {
+            if (!mbar_wait_bounded(&bars[warp][buf], phase[buf], 1u << 22)) {
                 failed = true;
                 break;
             }
@@ -389,7 +392,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
         if (lane == 0) atomicOr(P.error_flag, 1);
         // Do not leave with a bulk copy still writing this CTA's shared memory.
         for (int b = 0; b < 2; ++b)
-            if (pending[b]) mbar_wait_bounded(&bars[warp][b], phase[b], 1u << 24);
+            if (pending[b]) mbar_wait_bounded(&bars[warp][b], phase[b], 1u << 22);
     }
 }
 
