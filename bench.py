@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--flop-sample", type=int, default=20000)
+    p.add_argument("--envs", type=int, default=None, help="smaller case for profiling")
+    p.add_argument("--edges", type=int, default=None, help="smaller case for profiling")
     return p.parse_args()
 
 
@@ -151,8 +153,8 @@ def run_reference(args, world, rank):
     from bcc import workload
     if rank != 0:
         return
-    envs = workload.gen_envs(args.workload, seed=0)
-    edges = workload.gen_edges(args.workload, seed=0)
+    envs = workload.gen_envs(args.workload, args.envs, seed=0)
+    edges = workload.gen_edges(args.workload, args.edges, seed=0)
     N, E = envs.num_envs, len(edges)
     cfg = {"workload": "%s: panda, %d envs (U{8..64} primitives) x %d edges (log-uniform 0.05-2.0 rad)" % (
         args.workload, N, E), "envs": N, "edges": E, "resolution": 32}
@@ -211,8 +213,8 @@ def run_ours(args, world, rank, local, dist):
 
     dev = local
     torch.cuda.set_device(dev)
-    envs = workload.gen_envs(args.workload, seed=0)
-    edges = workload.gen_edges(args.workload, seed=rank)
+    envs = workload.gen_envs(args.workload, args.envs, seed=0)
+    edges = workload.gen_edges(args.workload, args.edges, seed=rank)
     N, E = envs.num_envs, len(edges)
     chk = Checker(dev)
     chk.upload(envs)
