@@ -52,7 +52,8 @@ struct bcc_ctx {
     // environment arena
     int num_envs = -1;
     int max_prims = 0;
-    DevBuf prims, env_off;
+    size_t blob_smem = 0;
+    DevBuf blobs, env_hdr;
     // per-call buffers
     DevBuf edges, steps, offs, table, row_edge, edge_self, swept, results, error_flag;
     int* h_total = nullptr;  // pinned readback of the sample-row total
@@ -210,18 +211,21 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     a.total_rows = total;
     a.table = ctx->table.as<float4>();
     a.row_edge = ctx->row_edge.as<int>();
-    a.prims = ctx->prims.as<float4>();
-    a.env_off = ctx->env_off.as<int>();
+    a.blobs = ctx->blobs.as<float4>();
+    a.env_hdr = ctx->env_hdr.as<float4>();
     a.num_envs = ctx->num_envs;
     a.max_prims = std::max(ctx->max_prims, 1);
+    a.blob_smem = ctx->blob_smem;
     a.d_results = d_results;
-    // Tile: warps per CTA limited by shared memory; environments per CTA.
+    // Tile: warps per CTA limited by shared memory; edges per CTA.
     int warps = 8;
-    while (warps > 1 && bcc::check_smem_bytes(a.max_prims, warps) > 200 * 1024) warps >>= 1;
-    if (bcc::check_smem_bytes(a.max_prims, warps) > 220 * 1024)
+    while (warps > 1 && bcc::check_smem_bytes(a.max_prims, a.blob_smem, warps) > 200 * 1024) warps >>= 1;
+    if (bcc::check_smem_bytes(a.max_prims, a.blob_smem, warps) > 220 * 1024)
         return fail(ctx, BCC_ERR_LIMIT, "an environment has too many primitives for shared-memory staging");
     a.warps = warps;
-    a.envs_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : 64, 1, 1 << 20);
+    a.edges_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : 128, 1, 1 << 20);
+    if ((E + a.edges_per_cta - 1) / a.edges_per_cta > 65535)
+        a.edges_per_cta = (E + 65534) / 65535;
     BCC_CUDA(ctx, bcc::launch_check(r, a, st));
     return BCC_OK;
 }
@@ -351,6 +355,83 @@ bcc_status pack(bcc_ctx* ctx, const bcc_env_soa* envs, std::vector<Rec>& recs, s
     return BCC_OK;
 }
 
+// Device arena: per environment a blob of its rounded-box records followed by
+// its interval-mask cull tables, and a 2 x float4 header.
+struct Arena {
+    std::vector<float> blob;     // concatenated blobs (float words, 16-byte granules)
+    std::vector<float> hdr;      // [N][8]
+    size_t max_blob_bytes = 0;
+};
+
+void build_arena(const std::vector<Rec>& recs, const std::vector<int>& off, Arena& A) {
+    const int N = (int)off.size() - 1;
+    constexpr int K = bcc::kGridSlabs;
+    constexpr int TRI = bcc::kGridTri;
+    A.blob.clear();
+    A.hdr.assign((size_t)N * 8, 0.0f);
+    for (int i = 0; i < N; ++i) {
+        const int p0 = off[i], np = off[i + 1] - off[i];
+        const int W = np > 0 ? (np + 63) / 64 : 0;
+        const size_t start = A.blob.size();  // in floats, multiple of 4
+        double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
+        for (int p = 0; p < np; ++p) {
+            const Rec& r = recs[p0 + p];
+            for (int k = 0; k < 20; ++k) A.blob.push_back(r.v[k]);
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = std::min(lo[a], (double)r.v[a] - r.v[16 + a]);
+                hi[a] = std::max(hi[a], (double)r.v[a] + r.v[16 + a]);
+            }
+        }
+        float inv[3] = {1.0f, 1.0f, 1.0f};
+        float org[3] = {0.0f, 0.0f, 0.0f};
+        if (np > 0) {
+            for (int a = 0; a < 3; ++a) {
+                const double width = (hi[a] - lo[a]) / K;
+                org[a] = (float)lo[a];
+                inv[a] = width > 1e-9 ? (float)(1.0 / width) : 1.0f;
+            }
+            // Slab range of each primitive, widened by 1e-5 m so that the FP32 slab
+            // arithmetic on the device can only over-include.
+            std::vector<int> s0(3 * (size_t)np), s1(3 * (size_t)np);
+            for (int p = 0; p < np; ++p) {
+                const Rec& r = recs[p0 + p];
+                for (int a = 0; a < 3; ++a) {
+                    const double l = ((double)r.v[a] - r.v[16 + a] - 1e-5 - org[a]) * inv[a];
+                    const double h = ((double)r.v[a] + r.v[16 + a] + 1e-5 - org[a]) * inv[a];
+                    s0[3 * p + a] = (int)std::min<double>(K - 1, std::max(0.0, std::floor(l)));
+                    s1[3 * p + a] = (int)std::min<double>(K - 1, std::max(0.0, std::floor(h)));
+                }
+            }
+            std::vector<uint64_t> m((size_t)3 * TRI * W, 0);
+            for (int a = 0; a < 3; ++a)
+                for (int i0 = 0; i0 < K; ++i0)
+                    for (int i1 = i0; i1 < K; ++i1) {
+                        uint64_t* dst = &m[((size_t)a * TRI + bcc::tri_index(i0, i1)) * W];
+                        for (int p = 0; p < np; ++p)
+                            if (s0[3 * p + a] <= i1 && s1[3 * p + a] >= i0) dst[p >> 6] |= 1ull << (p & 63);
+                    }
+            const size_t words = m.size() * 2;
+            const size_t at = A.blob.size();
+            A.blob.resize(at + words);
+            std::memcpy(&A.blob[at], m.data(), m.size() * sizeof(uint64_t));
+        }
+        const size_t bytes = (A.blob.size() - start) * sizeof(float);
+        A.max_blob_bytes = std::max(A.max_blob_bytes, bytes);
+        const uint32_t off16 = (uint32_t)(start / 4);  // float4 units
+        const uint32_t shape = (uint32_t)np | ((uint32_t)W << 16);
+        float* h = &A.hdr[(size_t)i * 8];
+        h[0] = org[0];
+        h[1] = org[1];
+        h[2] = org[2];
+        std::memcpy(&h[3], &off16, 4);
+        h[4] = inv[0];
+        h[5] = inv[1];
+        h[6] = inv[2];
+        std::memcpy(&h[7], &shape, 4);
+    }
+    if (A.blob.empty()) A.blob.assign(4, 0.0f);
+}
+
 }  // namespace
 
 extern "C" {
@@ -377,14 +458,21 @@ bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
     bcc_status s = pack(ctx, envs, recs, off, max_prims);
     if (s != BCC_OK) return s;
     const int N = envs->num_envs;
+    Arena A;
+    build_arena(recs, off, A);
+    const size_t blob_smem = (A.max_blob_bytes + 15) & ~(size_t)15;
+    if (blob_smem > 160 * 1024)
+        return fail(ctx, BCC_ERR_LIMIT, "an environment's primitives do not fit shared-memory staging (max ~1000)");
+    if (A.blob.size() / 4 > 0xffffffffull) return fail(ctx, BCC_ERR_LIMIT, "environment arena too large");
     BCC_CUDA(ctx, cudaSetDevice(ctx->device));
-    BCC_CUDA(ctx, ctx->prims.ensure(std::max<size_t>(1, recs.size()) * sizeof(Rec)));
-    BCC_CUDA(ctx, ctx->env_off.ensure(sizeof(int) * (N + 1)));
-    if (!recs.empty())
-        BCC_CUDA(ctx, cudaMemcpy(ctx->prims.p, recs.data(), recs.size() * sizeof(Rec), cudaMemcpyHostToDevice));
-    BCC_CUDA(ctx, cudaMemcpy(ctx->env_off.p, off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+    BCC_CUDA(ctx, ctx->blobs.ensure(A.blob.size() * sizeof(float)));
+    BCC_CUDA(ctx, ctx->env_hdr.ensure(std::max<size_t>(1, A.hdr.size()) * sizeof(float)));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->blobs.p, A.blob.data(), A.blob.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (N > 0)
+        BCC_CUDA(ctx, cudaMemcpy(ctx->env_hdr.p, A.hdr.data(), A.hdr.size() * sizeof(float), cudaMemcpyHostToDevice));
     ctx->num_envs = N;
     ctx->max_prims = max_prims;
+    ctx->blob_smem = blob_smem;
     return BCC_OK;
 }
 

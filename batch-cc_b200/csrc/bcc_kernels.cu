@@ -10,12 +10,16 @@
 //                          OR-reduced per edge; env-independent
 //   5. swept_kernel        per (edge, link) AABB of the link's bounding sphere over
 //                          all the edge's samples (cull volume)
-//   6. check_kernel        CTA = one edge x a tile of environments; each warp takes
-//                          one environment at a time: bulk-copies its primitives
-//                          into shared memory (cp.async.bulk + mbarrier, double
-//                          buffered), culls (primitive, link) pairs against the swept
-//                          AABBs, then walks (sample, pair) items 32 at a time in
-//                          check order with a warp-ballot exit on the first hit.
+//   6. check_kernel        CTA = one environment x a tile of edges.  The
+//                          environment's blob (primitive records + interval-mask
+//                          cull tables) is staged into shared memory once by a
+//                          cp.async.bulk copy and reused by every edge of the tile.
+//                          Each warp takes one edge at a time: lanes 0..9 turn the
+//                          link's swept AABB into three slab ranges and AND three
+//                          64-bit primitive masks (the cull), the surviving
+//                          (primitive, link) pairs are compacted, and the warp walks
+//                          (sample, pair) items 32 at a time in check order with a
+//                          warp-ballot exit on the first hit.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -52,14 +56,15 @@ static DevTables<M> host_tables() {
     for (int g = 0; g < M::num_env_groups; ++g) t.env_bound[g] = M::env_bound[g];
     for (int g = 0; g <= M::num_env_groups; ++g) t.leaf_begin[g] = M::env_leaf_begin[g];
     for (int i = 0; i < M::num_env_leaves; ++i) t.leaves[i] = M::env_leaves[i];
+    // Self tables hold sample-table row positions, not sphere indices.
     for (int g = 0; g < M::num_self_groups; ++g) {
-        t.self_bound[g][0] = M::self_bound[g][0];
-        t.self_bound[g][1] = M::self_bound[g][1];
+        t.self_bound[g][0] = M::table_pos[M::self_bound[g][0]];
+        t.self_bound[g][1] = M::table_pos[M::self_bound[g][1]];
     }
     for (int g = 0; g <= M::num_self_groups; ++g) t.self_pair_begin[g] = M::self_pair_begin[g];
     for (int i = 0; i < M::num_self_pairs; ++i) {
-        t.self_pairs[i][0] = M::self_pairs[i][0];
-        t.self_pairs[i][1] = M::self_pairs[i][1];
+        t.self_pairs[i][0] = (unsigned char)M::table_pos[M::self_pairs[i][0]];
+        t.self_pairs[i][1] = (unsigned char)M::table_pos[M::self_pairs[i][1]];
     }
     for (int s = 0; s < M::num_spheres; ++s) t.sphere_radius[s] = M::sphere_radius[s];
     return t;
@@ -132,7 +137,8 @@ template <class M, int S>
 struct WriteSpheres {
     __device__ __forceinline__ static void run(const Frames<M>& F, float4* __restrict__ out) {
         WriteSpheres<M, S - 1>::run(F, out);
-        out[S - 1] = fk_sphere<M, S - 1>(F);
+        constexpr int pos = M::table_pos[S - 1];
+        out[pos] = fk_sphere<M, S - 1>(F);
     }
 };
 template <class M>
@@ -140,8 +146,9 @@ struct WriteSpheres<M, 0> {
     __device__ __forceinline__ static void run(const Frames<M>&, float4*) {}
 };
 
-// Sample table row: num_spheres float4 (centre xyz, radius), one row per
-// (edge, sample) in edge order then sample index order.
+// Sample table row: num_spheres float4 (centre xyz, radius) in table_pos order
+// (env-group bounds, then env leaves, then the rest), one row per (edge,
+// sample) in edge order then sample index order.
 template <class M>
 __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges, int E,
                                                  const int* __restrict__ steps,
@@ -201,8 +208,8 @@ __global__ void __launch_bounds__(128) self_kernel(const float4* __restrict__ ta
 }
 
 // ------------------------------------------------------------------ 5. swept
-// One warp per edge: AABB (centre, half-size) of every env group's bounding
-// sphere over the edge's samples, inflated by radius + 0.005 + cull margin.
+// One warp per edge: AABB (lo, hi) of every env group's bounding sphere over
+// the edge's samples, inflated by radius + 0.005 + cull margin.
 template <class M>
 __global__ void swept_kernel(const float4* __restrict__ table, const int* __restrict__ offs, int E,
                              float4* __restrict__ swept) {
@@ -212,7 +219,7 @@ __global__ void swept_kernel(const float4* __restrict__ table, const int* __rest
     const int r0 = offs[warp], r1 = offs[warp + 1];
     const DevTables<M>& T = tab<M>();
     for (int g = 0; g < M::num_env_groups; ++g) {
-        const int b = T.env_bound[g];
+        const int b = g;  // bounds lead every table row
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int r = r0 + lane; r < r1; r += 32) {
             const float4 c = table[(size_t)r * M::num_spheres + b];
@@ -228,120 +235,106 @@ __global__ void swept_kernel(const float4* __restrict__ table, const int* __rest
             }
         }
         if (lane == 0) {
-            const float pad = T.sphere_radius[b] + kEnvInflate + kCullMargin;
-            float4 c, h;
-            c.x = 0.5f * (lo[0] + hi[0]); c.y = 0.5f * (lo[1] + hi[1]); c.z = 0.5f * (lo[2] + hi[2]);
-            h.x = 0.5f * (hi[0] - lo[0]) + pad; h.y = 0.5f * (hi[1] - lo[1]) + pad;
-            h.z = 0.5f * (hi[2] - lo[2]) + pad;
-            c.w = 0.0f; h.w = 0.0f;
-            swept[((size_t)warp * M::num_env_groups + g) * 2 + 0] = c;
+            const float pad = T.sphere_radius[T.env_bound[g]] + kEnvInflate + kCullMargin;
+            const float4 l = make_float4(lo[0] - pad, lo[1] - pad, lo[2] - pad, 0.0f);
+            const float4 h = make_float4(hi[0] + pad, hi[1] + pad, hi[2] + pad, 0.0f);
+            swept[((size_t)warp * M::num_env_groups + g) * 2 + 0] = l;
             swept[((size_t)warp * M::num_env_groups + g) * 2 + 1] = h;
         }
     }
 }
 
 // ------------------------------------------------------------------ 6. check
-struct CheckSmemLayout {
-    int max_prims;  // per environment, rounded up
-    __host__ __device__ size_t prim_bytes() const { return (size_t)max_prims * kPrimF4 * 16; }
-    __host__ __device__ size_t pair_bytes() const { return (((size_t)max_prims * 16 * 2) + 15) & ~(size_t)15; }
-    __host__ __device__ size_t per_warp() const { return 2 * prim_bytes() + pair_bytes(); }
-};
+// Slab index range of [lo, hi] on one axis of an environment's cull grid, as a
+// triangular table index; -1 when the interval misses every primitive.
+__device__ __forceinline__ int slab_tri(float lo, float hi, float g0, float inv) {
+    const float f0 = (lo - g0) * inv, f1 = (hi - g0) * inv;
+    if (!(f1 >= 0.0f) || !(f0 < (float)kGridSlabs)) return -1;
+    const int i0 = (int)fminf(fmaxf(floorf(f0), 0.0f), (float)(kGridSlabs - 1));
+    const int i1 = (int)fminf(fmaxf(floorf(f1), 0.0f), (float)(kGridSlabs - 1));
+    return tri_index(i0, i1);
+}
 
 template <class M, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
+    constexpr int G = M::num_env_groups;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bars[WARPS][2];
-    __shared__ float4 s_swept[M::num_env_groups][2];
+    __shared__ uint64_t bar;
 
-    const int e = blockIdx.y;
-    const int tile0 = blockIdx.x * P.envs_per_cta;
-    const int tile1 = min(tile0 + P.envs_per_cta, P.num_envs);
+    const int env = blockIdx.x;
+    const int e_begin = blockIdx.y * P.edges_per_cta;
+    const int e_end = min(e_begin + P.edges_per_cta, P.num_edges);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    // Self-colliding edge: every environment's verdict is "collision".
-    if (P.edge_self[e]) {
-        for (int v = tile0 + threadIdx.x; v < tile1; v += blockDim.x)
-            P.results[(size_t)e * P.num_envs + v] = 1;
-        return;
-    }
-    if (threadIdx.x < M::num_env_groups * 2)
-        (&s_swept[0][0])[threadIdx.x] = P.swept[(size_t)e * M::num_env_groups * 2 + threadIdx.x];
-    if (lane == 0) {
-        mbar_init(&bars[warp][0], 1);
-        mbar_init(&bars[warp][1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
+    // Environment header: grid origin, inverse slab width, blob offset and shape.
+    const float4 h0 = P.env_hdr[2 * env + 0];
+    const float4 h1 = P.env_hdr[2 * env + 1];
+    const uint32_t blob_off = __float_as_uint(h0.w);
+    const uint32_t shape = __float_as_uint(h1.w);
+    const int np = (int)(shape & 0xffffu);
+    const int W = (int)(shape >> 16);  // 64-bit words per primitive mask
+    const uint32_t blob_bytes = (uint32_t)np * kPrimF4 * 16u + 3u * kGridTri * (uint32_t)W * 8u;
 
-    const CheckSmemLayout L{P.max_prims};
-    unsigned char* wbase = smem + (size_t)warp * L.per_warp();
-    float4* pbuf[2] = {reinterpret_cast<float4*>(wbase), reinterpret_cast<float4*>(wbase + L.prim_bytes())};
-    uint16_t* pairs = reinterpret_cast<uint16_t*>(wbase + 2 * L.prim_bytes());
+    const float4* prim = reinterpret_cast<const float4*>(smem);
+    const uint64_t* masks = reinterpret_cast<const uint64_t*>(smem + (size_t)np * kPrimF4 * 16);
+    uint16_t* pairs = reinterpret_cast<uint16_t*>(smem + P.blob_smem) + (size_t)warp * P.pairs_per_warp;
 
-    const int n = P.steps[e];
-    const int S = kLanes * n;
-    const size_t row0 = (size_t)P.offs[e];
+    bool ok = true;
+    if (np > 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)blob_off, blob_bytes, &bar);
+        ok = mbar_wait_bounded(&bar, 0u, 1u << 22);
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
+            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
+            return;
+        }
+    }
     const DevTables<M>& T = tab<M>();
 
-    // Per-buffer mbarrier phase; pending = a bulk copy was issued and not yet waited on.
-    uint32_t phase[2] = {0u, 0u};
-    bool pending[2] = {false, false};
-    int v = tile0 + warp;
-    auto issue = [&](int env, int b) {
-        const int p0 = P.env_off[env], p1 = P.env_off[env + 1];
-        const uint32_t bytes = (uint32_t)(p1 - p0) * kPrimF4 * 16u;
-        if (bytes) {
-            if (lane == 0) bulk_copy_g2s(pbuf[b], P.prims + (size_t)p0 * kPrimF4, bytes, &bars[warp][b]);
-            pending[b] = true;
+    for (int e = e_begin + warp; e < e_end; e += WARPS) {
+        uint8_t* out = P.results + (size_t)e * P.num_envs + env;
+        if (np == 0) {
+            if (lane == 0) *out = P.edge_self[e] ? 1 : 0;
+            continue;
         }
-    };
-    if (v < tile1) issue(v, 0);
-    int buf = 0;
-    bool failed = false;
-    for (; v < tile1; v += WARPS, buf ^= 1) {
-        const int nv = v + WARPS;
-        __syncwarp();
-        if (nv < tile1) issue(nv, buf ^ 1);
-        if (pending[buf]) {
-            if (!mbar_wait_bounded(&bars[warp][buf], phase[buf], 1u << 22)) {
-                failed = true;
-                break;
-            }
-            phase[buf] ^= 1u;
-            pending[buf] = false;
+        if (P.edge_self[e]) {  // a self-colliding sample collides in every environment
+            if (lane == 0) *out = 1;
+            continue;
         }
-        const int np = P.env_off[v + 1] - P.env_off[v];
-        const float4* prim = pbuf[buf];
-
-        // Cull: (primitive, link) pairs whose AABBs overlap; compact into `pairs`.
+        // Cull: lane g < G intersects link g's swept box with the env's slab tables.
+        int tx = -1, ty = -1, tz = -1;
+        if (lane < G) {
+            const float4 lo = P.swept[((size_t)e * G + lane) * 2 + 0];
+            const float4 hi = P.swept[((size_t)e * G + lane) * 2 + 1];
+            tx = slab_tri(lo.x, hi.x, h0.x, h1.x);
+            ty = slab_tri(lo.y, hi.y, h0.y, h1.y);
+            tz = slab_tri(lo.z, hi.z, h0.z, h1.z);
+        }
+        const bool live = tx >= 0 && ty >= 0 && tz >= 0;
         int C = 0;
-        for (int p0 = 0; p0 < np; p0 += 32) {
-            const int p = p0 + lane;
-            uint32_t mask = 0;
-            if (p < np) {
-                const float4 c = prim[p * kPrimF4 + 0];
-                const float4 h = prim[p * kPrimF4 + 4];
-#pragma unroll
-                for (int g = 0; g < M::num_env_groups; ++g) {
-                    const float4 sc = s_swept[g][0], sh = s_swept[g][1];
-                    const bool ov = fabsf(c.x - sc.x) <= h.x + sh.x && fabsf(c.y - sc.y) <= h.y + sh.y &&
-                                    fabsf(c.z - sc.z) <= h.z + sh.z;
-                    mask |= (uint32_t)ov << g;
-                }
+        for (int w = 0; w < W; ++w) {
+            uint64_t m = 0;
+            if (live) {
+                m = masks[((size_t)0 * kGridTri + tx) * W + w] & masks[((size_t)1 * kGridTri + ty) * W + w] &
+                    masks[((size_t)2 * kGridTri + tz) * W + w];
             }
-            const int cnt = __popc(mask);
+            const int cnt = __popcll(m);
             int x = cnt;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += y;
             }
-            int w = C + x - cnt;
-            while (mask) {
-                const int g = __ffs(mask) - 1;
-                mask &= mask - 1;
-                pairs[w++] = (uint16_t)((p << 4) | g);
+            int pos = C + x - cnt;
+            while (m) {
+                const int b = __ffsll((long long)m) - 1;
+                m &= m - 1;
+                pairs[pos++] = (uint16_t)(((w * 64 + b) << 4) | lane);
             }
             C += __shfl_sync(0xffffffffu, x, 31);
         }
@@ -350,7 +343,9 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
         // Walk (sample rank, pair) items, 32 per step, in check order.
         bool collide = false;
         if (C > 0) {
-            const int total = S * C;
+            const int n = P.steps[e];
+            const int total = kLanes * n * C;
+            const size_t row0 = (size_t)P.offs[e];
             const int dr = 32 / C, dc = 32 % C;
             int r = lane / C, c = lane - (lane / C) * C;
             for (int w0 = 0; w0 < total; w0 += 32) {
@@ -361,11 +356,11 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
                     const int p = (int)(pr >> 4), g = (int)(pr & 15u);
                     const float4* rec = prim + p * kPrimF4;
                     const float4* row = P.table + (row0 + (size_t)k) * M::num_spheres;
-                    float4 bs = row[T.env_bound[g]];
+                    float4 bs = row[g];
                     bs.w += kEnvInflate;
                     if (sphere_hits_prim(bs, rec)) {
                         for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1]; ++li) {
-                            float4 ls = row[T.leaves[li]];
+                            float4 ls = row[G + li];
                             ls.w += kEnvInflate;
                             if (sphere_hits_prim(ls, rec)) {
                                 hit = true;
@@ -386,20 +381,15 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
                 }
             }
         }
-        if (lane == 0) P.results[(size_t)e * P.num_envs + v] = collide ? 1 : 0;
-    }
-    if (failed) {
-        if (lane == 0) atomicOr(P.error_flag, 1);
-        // Do not leave with a bulk copy still writing this CTA's shared memory.
-        for (int b = 0; b < 2; ++b)
-            if (pending[b]) mbar_wait_bounded(&bars[warp][b], phase[b], 1u << 22);
+        __syncwarp();
+        if (lane == 0) *out = collide ? 1 : 0;
     }
 }
 
 // ------------------------------------------------------------------ launchers
-size_t check_smem_bytes(int max_prims, int warps) {
-    CheckSmemLayout L{max_prims};
-    return L.per_warp() * warps;
+size_t check_smem_bytes(int max_prims, size_t blob_smem, int warps) {
+    const size_t ppw = (size_t)((max_prims * 16 + 7) & ~7);
+    return blob_smem + (size_t)warps * ppw * sizeof(uint16_t);
 }
 
 template <class M>
@@ -412,12 +402,13 @@ static cudaError_t run_steps(const PipelineArgs& a, cudaStream_t st) {
 }
 
 template <class M, int W>
-static cudaError_t launch_check_w(const CheckParams& P, int E, cudaStream_t st) {
-    const size_t smem = check_smem_bytes(P.max_prims, W);
+static cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st) {
+    P.pairs_per_warp = (P.max_prims * M::num_env_groups + 7) & ~7;
+    const size_t smem = P.blob_smem + (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
     cudaError_t err = cudaFuncSetAttribute(check_kernel<M, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
     if (err != cudaSuccess) return err;
-    dim3 grid((P.num_envs + P.envs_per_cta - 1) / P.envs_per_cta, E);
+    dim3 grid(P.num_envs, (E + P.edges_per_cta - 1) / P.edges_per_cta);
     check_kernel<M, W><<<grid, W * 32, smem, st>>>(P);
     return cudaGetLastError();
 }
@@ -440,11 +431,13 @@ static cudaError_t run_check(const PipelineArgs& a, cudaStream_t st) {
     if (ev) cudaEventRecord(ev[4], st);
 
     CheckParams P;
-    P.prims = a.prims;
-    P.env_off = a.env_off;
+    P.blobs = a.blobs;
+    P.env_hdr = a.env_hdr;
     P.num_envs = a.num_envs;
+    P.num_edges = E;
     P.max_prims = a.max_prims;
-    P.envs_per_cta = a.envs_per_cta;
+    P.blob_smem = a.blob_smem;
+    P.edges_per_cta = a.edges_per_cta;
     P.steps = a.steps;
     P.offs = a.offs;
     P.table = a.table;

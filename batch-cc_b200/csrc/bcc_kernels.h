@@ -7,12 +7,26 @@
 
 namespace bcc {
 
+// Cull grid of an environment: kGridSlabs slabs per axis between the min and
+// max of its primitives' AABBs; for every slab range [i0, i1] (triangular
+// index) a bit mask of the primitives whose AABB meets that range.
+constexpr int kGridSlabs = 16;
+constexpr int kGridTri = kGridSlabs * (kGridSlabs + 1) / 2;
+
+__host__ __device__ __forceinline__ int tri_index(int i0, int i1) {
+    return i0 * kGridSlabs - (i0 * (i0 - 1)) / 2 + (i1 - i0);
+}
+
 struct CheckParams {
-    const float4* prims;     // [total prims][5] rounded-box records
-    const int* env_off;      // [num_envs + 1] first primitive of each env
+    const float4* blobs;     // per env: [np][5] rounded-box records, then 3 x kGridTri x W masks
+    const float4* env_hdr;   // [num_envs][2]: (grid origin xyz, blob offset in float4s),
+                             //                 (1/slab width xyz, np | W << 16)
     int num_envs;
-    int max_prims;           // max primitives of one env (shared-memory sizing)
-    int envs_per_cta;
+    int num_edges;
+    int max_prims;           // max primitives of one env (pair-list sizing)
+    size_t blob_smem;        // bytes of the largest env blob (16-byte multiple)
+    int pairs_per_warp;
+    int edges_per_cta;
     const int* steps;        // [E] n per edge
     const int* offs;         // [E + 1] first sample row of each edge
     const float4* table;     // [rows][num_spheres] sphere centres + radius
@@ -33,11 +47,12 @@ struct PipelineArgs {
     int* row_edge;           // [total_rows]
     int* edge_self;          // [E]
     float4* swept;           // [E][groups][2]
-    const float4* prims;
-    const int* env_off;
+    const float4* blobs;
+    const float4* env_hdr;
     int num_envs;
     int max_prims;
-    int envs_per_cta;
+    size_t blob_smem;
+    int edges_per_cta;
     int warps;               // warps per check CTA (8, 4, 2 or 1)
     uint8_t* d_results;
     int* error_flag;
@@ -49,7 +64,7 @@ cudaError_t upload_robot_tables(int robot);
 cudaError_t launch_steps(int robot, const PipelineArgs& a, cudaStream_t st);
 // Stage 2: FK table, self-collision, swept volumes, environment check.
 cudaError_t launch_check(int robot, const PipelineArgs& a, cudaStream_t st);
-size_t check_smem_bytes(int max_prims, int warps);
+size_t check_smem_bytes(int max_prims, size_t blob_smem, int warps);
 int robot_num_spheres(int robot);
 int robot_num_env_groups(int robot);
 int robot_dof(int robot);

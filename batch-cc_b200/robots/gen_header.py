@@ -111,6 +111,18 @@ def main():
         w("        %s," % ", ".join(flat[i:i + 12]))
     w("    };")
     w("")
+    # Sample-table row order: env-group bounds first (group order), then the
+    # env-checked leaves in env_leaves order, then every other sphere.
+    order = [g["bound"] for g in env] + [i for g in env for i in g["leaves"]]
+    order += [i for i in range(len(sph)) if i not in order]
+    pos = [0] * len(sph)
+    for k, i in enumerate(order):
+        pos[i] = k
+    w("    // Position of sphere k in a sample-table row: the env-group bounding spheres")
+    w("    // first (group order), then the env-checked leaves (env_leaves order), then")
+    w("    // the rest; so a sample's bounds are contiguous and leaf j sits at groups + j.")
+    w("    static constexpr int table_pos[%d] = {%s};" % (len(sph), ", ".join(map(str, pos))))
+    w("")
     w("    // Joint-limit scale of the robot description: q = u * s_m + s_a.")
     w("    static constexpr float s_m[%d] = {%s};" % (dof, ", ".join(repr(float(np.float32(v))) + "f" for v in s_m)))
     w("    static constexpr float s_a[%d] = {%s};" % (dof, ", ".join(repr(float(np.float32(v))) + "f" for v in s_a)))
