@@ -298,12 +298,9 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
 
     for (int e = e_begin + warp; e < e_end; e += WARPS) {
         uint8_t* out = P.results + (size_t)e * P.num_envs + env;
-        if (np == 0) {
-            if (lane == 0) *out = P.edge_self[e] ? 1 : 0;
-            continue;
-        }
-        if (P.edge_self[e]) {  // a self-colliding sample collides in every environment
-            if (lane == 0) *out = 1;
+        const int self = P.edge_self[e];
+        if (np == 0 || self) {  // a self-colliding sample collides in every environment
+            if (lane == 0) *out = self ? 1 : 0;
             continue;
         }
         // Cull: lane g < G intersects link g's swept box with the env's slab tables.
@@ -316,27 +313,27 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
             tz = slab_tri(lo.z, hi.z, h0.z, h1.z);
         }
         const bool live = tx >= 0 && ty >= 0 && tz >= 0;
+        // Compact the surviving (primitive, link) pairs, link-major: for each link
+        // the whole warp writes that link's mask bits, lane l owning bits l, l + 32.
         int C = 0;
+        const uint32_t lt = (1u << lane) - 1u;
         for (int w = 0; w < W; ++w) {
-            uint64_t m = 0;
+            uint64_t mine = 0;
             if (live) {
-                m = masks[((size_t)0 * kGridTri + tx) * W + w] & masks[((size_t)1 * kGridTri + ty) * W + w] &
-                    masks[((size_t)2 * kGridTri + tz) * W + w];
+                mine = masks[((size_t)0 * kGridTri + tx) * W + w] & masks[((size_t)1 * kGridTri + ty) * W + w] &
+                       masks[((size_t)2 * kGridTri + tz) * W + w];
             }
-            const int cnt = __popcll(m);
-            int x = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
+#pragma unroll 1
+            for (int g = 0; g < G; ++g) {
+                const uint32_t mlo = __shfl_sync(0xffffffffu, (uint32_t)mine, g);
+                const uint32_t mhi = __shfl_sync(0xffffffffu, (uint32_t)(mine >> 32), g);
+                if ((mlo | mhi) == 0u) continue;
+                const int clo = __popc(mlo);
+                if ((mlo >> lane) & 1u) pairs[C + __popc(mlo & lt)] = (uint16_t)(((w * 64 + lane) << 4) | g);
+                if ((mhi >> lane) & 1u)
+                    pairs[C + clo + __popc(mhi & lt)] = (uint16_t)(((w * 64 + 32 + lane) << 4) | g);
+                C += clo + __popc(mhi);
             }
-            int pos = C + x - cnt;
-            while (m) {
-                const int b = __ffsll((long long)m) - 1;
-                m &= m - 1;
-                pairs[pos++] = (uint16_t)(((w * 64 + b) << 4) | lane);
-            }
-            C += __shfl_sync(0xffffffffu, x, 31);
         }
         __syncwarp();
 
@@ -349,29 +346,40 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
             const int dr = 32 / C, dc = 32 % C;
             int r = lane / C, c = lane - (lane / C) * C;
             for (int w0 = 0; w0 < total; w0 += 32) {
-                bool hit = false;
+                bool gate = false;
+                const float4* rec = prim;
+                const float4* row = P.table;
+                int g = 0;
                 if (w0 + lane < total) {
                     const int k = reference_rank_to_sample(r, n);
                     const uint32_t pr = pairs[c];
-                    const int p = (int)(pr >> 4), g = (int)(pr & 15u);
-                    const float4* rec = prim + p * kPrimF4;
-                    const float4* row = P.table + (row0 + (size_t)k) * M::num_spheres;
+                    g = (int)(pr & 15u);
+                    rec = prim + (int)(pr >> 4) * kPrimF4;
+                    row = P.table + (row0 + (size_t)k) * M::num_spheres;
                     float4 bs = row[g];
                     bs.w += kEnvInflate;
-                    if (sphere_hits_prim(bs, rec)) {
-                        for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1]; ++li) {
+                    gate = sphere_hits_prim(bs, rec);
+                }
+                if (__any_sync(0xffffffffu, gate)) {
+                    // Leaves of every gated item, one leaf per lane per step; the warp
+                    // stops at the first step in which any lane's leaf hits.
+                    int li = gate ? T.leaf_begin[g] : 0;
+                    const int le = gate ? T.leaf_begin[g + 1] : 0;
+                    for (;;) {
+                        bool hit = false;
+                        if (li < le) {
                             float4 ls = row[G + li];
                             ls.w += kEnvInflate;
-                            if (sphere_hits_prim(ls, rec)) {
-                                hit = true;
-                                break;
-                            }
+                            hit = sphere_hits_prim(ls, rec);
                         }
+                        ++li;
+                        if (__any_sync(0xffffffffu, hit)) {
+                            collide = true;
+                            break;
+                        }
+                        if (!__any_sync(0xffffffffu, li < le)) break;
                     }
-                }
-                if (__any_sync(0xffffffffu, hit)) {
-                    collide = true;
-                    break;
+                    if (collide) break;
                 }
                 c += dc;
                 r += dr;
