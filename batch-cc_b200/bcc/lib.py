@@ -61,6 +61,7 @@ def lib():
         L.bcc_robot_dof.argtypes = [ctypes.c_int]
         L.bcc_measure_fp32_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
         L.bcc_set_profiling.argtypes = [vp, ctypes.c_int32]
+        L.bcc_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]
         L.bcc_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
         L.bcc_pack_envs.argtypes = [ctypes.POINTER(BccEnvSoa), ctypes.POINTER(ctypes.c_float),
                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64),
@@ -73,7 +74,7 @@ def exported_symbols():
     """Names declared in include/bcc.h (checked against the .so by the tests)."""
     return ["bcc_create", "bcc_destroy", "bcc_last_error", "bcc_upload_envs", "bcc_check",
             "bcc_check_device", "bcc_edge_samples", "bcc_robot_dof", "bcc_pack_envs",
-            "bcc_set_profiling", "bcc_stage_times", "bcc_measure_fp32_peak"]
+            "bcc_set_profiling", "bcc_stage_times", "bcc_measure_fp32_peak", "bcc_work_counters"]
 
 
 def make_opts(order="plain", use_graph=False, tile=0):
@@ -125,8 +126,16 @@ class Checker:
         self._raise(st)
         return out
 
-    def set_profiling(self, on=True):
-        self._raise(lib().bcc_set_profiling(self._h, int(on)))
+    def set_profiling(self, on=True, counters=False):
+        self._raise(lib().bcc_set_profiling(self._h, (1 if on else 0) | (2 if counters else 0)))
+
+    COUNTERS = ("pairs", "candidates", "chunks", "gate_chunks", "leaf_steps", "colliding")
+
+    def work_counters(self):
+        out = (ctypes.c_uint64 * 6)()
+        if lib().bcc_work_counters(self._h, out, 6) < 0:
+            raise BccError(1, "work counters are off or no check has run")
+        return dict(zip(self.COUNTERS, [int(v) for v in out]))
 
     STAGES = ("steps", "fk", "self", "swept", "check")
 

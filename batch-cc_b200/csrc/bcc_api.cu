@@ -58,6 +58,8 @@ struct bcc_ctx {
     DevBuf edges, steps, offs, table, row_edge, edge_self, swept, results, error_flag;
     int* h_total = nullptr;  // pinned readback of the sample-row total
     bool profiling = false;
+    bool counting = false;
+    DevBuf counters;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -197,6 +199,12 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     a.swept = ctx->swept.as<float4>();
     a.error_flag = ctx->error_flag.as<int>();
     a.stage_events = ctx->profiling ? ctx->ev : nullptr;
+    a.counters = nullptr;
+    if (ctx->counting) {
+        BCC_CUDA(ctx, ctx->counters.ensure(sizeof(unsigned long long) * bcc::kNumCounters));
+        a.counters = ctx->counters.as<unsigned long long>();
+        BCC_CUDA(ctx, cudaMemsetAsync(a.counters, 0, sizeof(unsigned long long) * bcc::kNumCounters, st));
+    }
     BCC_CUDA(ctx, cudaMemsetAsync(a.error_flag, 0, sizeof(int), st));
     BCC_CUDA(ctx, bcc::launch_steps(r, a, st));
     BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.offs + E, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -269,7 +277,17 @@ bcc_status bcc_set_profiling(bcc_ctx* ctx, int32_t on) {
     for (auto& e : ctx->ev)
         if (!e) BCC_CUDA(ctx, cudaEventCreate(&e));
     ctx->profiling = on != 0;
+    ctx->counting = (on & 2) != 0;
     return BCC_OK;
+}
+
+int32_t bcc_work_counters(bcc_ctx* ctx, uint64_t* out, int32_t max_counters) {
+    if (!ctx || !out || !ctx->counting || !ctx->counters.p) return -1;
+    const int n = std::min<int>(max_counters, bcc::kNumCounters);
+    unsigned long long tmp[bcc::kNumCounters];
+    if (cudaMemcpy(tmp, ctx->counters.p, sizeof(tmp), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    for (int i = 0; i < n; ++i) out[i] = tmp[i];
+    return n;
 }
 
 int32_t bcc_stage_times(bcc_ctx* ctx, float* ms, int32_t max_stages) {

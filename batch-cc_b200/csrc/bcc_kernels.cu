@@ -339,6 +339,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
 
         // Walk (sample rank, pair) items, 32 per step, in check order.
         bool collide = false;
+        unsigned long long n_chunks = 0, n_gates = 0, n_leaf = 0;
         if (C > 0) {
             const int n = P.steps[e];
             const int total = kLanes * n * C;
@@ -360,7 +361,9 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
                     bs.w += kEnvInflate;
                     gate = sphere_hits_prim(bs, rec);
                 }
+                ++n_chunks;
                 if (__any_sync(0xffffffffu, gate)) {
+                    ++n_gates;
                     // Leaves of every gated item, one leaf per lane per step; the warp
                     // stops at the first step in which any lane's leaf hits.
                     int li = gate ? T.leaf_begin[g] : 0;
@@ -373,6 +376,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
                             hit = sphere_hits_prim(ls, rec);
                         }
                         ++li;
+                        ++n_leaf;
                         if (__any_sync(0xffffffffu, hit)) {
                             collide = true;
                             break;
@@ -390,7 +394,17 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
             }
         }
         __syncwarp();
-        if (lane == 0) *out = collide ? 1 : 0;
+        if (lane == 0) {
+            *out = collide ? 1 : 0;
+            if (P.counters) {
+                atomicAdd(P.counters + 0, 1ull);
+                atomicAdd(P.counters + 1, (unsigned long long)C);
+                atomicAdd(P.counters + 2, n_chunks);
+                atomicAdd(P.counters + 3, n_gates);
+                atomicAdd(P.counters + 4, n_leaf);
+                atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
+            }
+        }
     }
 }
 
@@ -453,6 +467,7 @@ static cudaError_t run_check(const PipelineArgs& a, cudaStream_t st) {
     P.edge_self = a.edge_self;
     P.results = a.d_results;
     P.error_flag = a.error_flag;
+    P.counters = a.counters;
     switch (a.warps) {
         case 8: err = launch_check_w<M, 8>(P, E, st); break;
         case 4: err = launch_check_w<M, 4>(P, E, st); break;

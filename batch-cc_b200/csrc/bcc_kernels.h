@@ -34,7 +34,13 @@ struct CheckParams {
     const int* edge_self;    // [E] 1 when some sample self-collides
     uint8_t* results;        // [E][num_envs]
     int* error_flag;         // set when a bounded wait gives up
+    unsigned long long* counters;  // null, or kNumCounters work counters (diagnostics)
 };
+
+// Work counters of the environment check (diagnostics, off by default):
+// pairs walked, candidate (primitive, link) pairs, 32-item chunks, gate steps
+// with a hit, leaf steps, colliding pairs.
+constexpr int kNumCounters = 6;
 
 struct PipelineArgs {
     const float* d_edges;    // [E][2][dof]
@@ -57,6 +63,7 @@ struct PipelineArgs {
     uint8_t* d_results;
     int* error_flag;
     cudaEvent_t* stage_events;  // null, or 6 events bracketing the 5 stages
+    unsigned long long* counters;
 };
 
 cudaError_t upload_robot_tables(int robot);

@@ -142,6 +142,15 @@ bcc_status bcc_pack_envs(const bcc_env_soa* envs, float* records, int32_t* env_o
 bcc_status bcc_set_profiling(bcc_ctx* ctx, int32_t on);
 int32_t bcc_stage_times(bcc_ctx* ctx, float* ms, int32_t max_stages);
 
+/*
+ * Work counters of the last check, when profiling was switched on with bit 1
+ * set (bcc_set_profiling(ctx, 3)): [0] pairs walked, [1] candidate
+ * (primitive, link) pairs after the cull, [2] 32-item chunks, [3] chunks with a
+ * gate hit, [4] leaf steps, [5] colliding pairs.  Diagnostics only: counting
+ * adds atomics to the check kernel.  Returns the number written, or -1.
+ */
+int32_t bcc_work_counters(bcc_ctx* ctx, uint64_t* out, int32_t max_counters);
+
 /* Diagnostics: FP32 FMA-pipe throughput of `device` in TFLOP/s, measured by a
  * short probe kernel (the roofline denominator of the scalar-FP32 checker). */
 bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
