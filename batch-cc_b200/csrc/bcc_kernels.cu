@@ -348,40 +348,57 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
             int r = lane / C, c = lane - (lane / C) * C;
             for (int w0 = 0; w0 < total; w0 += 32) {
                 bool gate = false;
-                const float4* rec = prim;
-                const float4* row = P.table;
-                int g = 0;
+                int g = 0, p = 0, k = 0;
                 if (w0 + lane < total) {
-                    const int k = reference_rank_to_sample(r, n);
+                    k = reference_rank_to_sample(r, n);
                     const uint32_t pr = pairs[c];
                     g = (int)(pr & 15u);
-                    rec = prim + (int)(pr >> 4) * kPrimF4;
-                    row = P.table + (row0 + (size_t)k) * M::num_spheres;
-                    float4 bs = row[g];
+                    p = (int)(pr >> 4);
+                    float4 bs = P.table[(row0 + (size_t)k) * M::num_spheres + g];
                     bs.w += kEnvInflate;
-                    gate = sphere_hits_prim(bs, rec);
+                    gate = sphere_hits_prim(bs, prim + p * kPrimF4);
                 }
                 ++n_chunks;
                 if (__any_sync(0xffffffffu, gate)) {
                     ++n_gates;
-                    // Leaves of every gated item, one leaf per lane per step; the warp
-                    // stops at the first step in which any lane's leaf hits.
-                    int li = gate ? T.leaf_begin[g] : 0;
-                    const int le = gate ? T.leaf_begin[g + 1] : 0;
-                    for (;;) {
-                        bool hit = false;
-                        if (li < le) {
-                            float4 ls = row[G + li];
-                            ls.w += kEnvInflate;
-                            hit = sphere_hits_prim(ls, rec);
+                    // Leaf work of every gated item, flattened over the warp: item j owns
+                    // leaf slots [incl_j - cnt_j, incl_j); each step tests 32 slots and the
+                    // warp stops at the first step with a hit.
+                    const int cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
+                    int incl = cnt;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    const int L = __shfl_sync(0xffffffffu, incl, 31);
+                    const int first = T.leaf_begin[g];
+                    for (int t0 = 0; t0 < L; t0 += 32) {
+                        const int t = t0 + lane;
+                        // owner j: the first lane whose inclusive count exceeds t
+                        int j = 0;
+#pragma unroll
+                        for (int step = 16; step; step >>= 1) {
+                            const int v = __shfl_sync(0xffffffffu, incl, j + step - 1);
+                            if (v <= t) j += step;
                         }
-                        ++li;
+                        const int j_incl = __shfl_sync(0xffffffffu, incl, j);
+                        const int j_cnt = __shfl_sync(0xffffffffu, cnt, j);
+                        const int j_first = __shfl_sync(0xffffffffu, first, j);
+                        const int j_k = __shfl_sync(0xffffffffu, k, j);
+                        const int j_p = __shfl_sync(0xffffffffu, p, j);
+                        bool hit = false;
+                        if (t < L) {
+                            const int leaf = j_first + (t - (j_incl - j_cnt));
+                            float4 ls = P.table[(row0 + (size_t)j_k) * M::num_spheres + G + leaf];
+                            ls.w += kEnvInflate;
+                            hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
+                        }
                         ++n_leaf;
                         if (__any_sync(0xffffffffu, hit)) {
                             collide = true;
                             break;
                         }
-                        if (!__any_sync(0xffffffffu, li < le)) break;
                     }
                     if (collide) break;
                 }

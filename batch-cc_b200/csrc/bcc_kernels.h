@@ -10,7 +10,7 @@ namespace bcc {
 // Cull grid of an environment: kGridSlabs slabs per axis between the min and
 // max of its primitives' AABBs; for every slab range [i0, i1] (triangular
 // index) a bit mask of the primitives whose AABB meets that range.
-constexpr int kGridSlabs = 16;
+constexpr int kGridSlabs = 32;
 constexpr int kGridTri = kGridSlabs * (kGridSlabs + 1) / 2;
 
 __host__ __device__ __forceinline__ int tri_index(int i0, int i1) {
