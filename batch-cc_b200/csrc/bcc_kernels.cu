@@ -96,40 +96,43 @@ __global__ void edge_steps_kernel(const float* __restrict__ edges, int E, int re
 
 // ------------------------------------------------------------------ 2. scan
 // Single-CTA exclusive scan of 32*steps[e] into offs[e], offs[E] = total.
+// Sums run in 64 bits and every offset saturates at INT32_MAX, so a total too
+// large for the sample table can never wrap into a small, valid-looking one;
+// the host rejects any total above its limit.
 __global__ void scan_kernel(const int* __restrict__ steps, int E, int* __restrict__ offs) {
-    __shared__ int warp_sums[32];
-    __shared__ int carry;
+    __shared__ long long warp_sums[32];
+    __shared__ long long carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int base = 0; base < E; base += blockDim.x) {
         const int i = base + threadIdx.x;
-        int v = (i < E) ? kLanes * steps[i] : 0;
-        int x = v;
+        const long long v = (i < E) ? (long long)kLanes * steps[i] : 0;
+        long long x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
+            const long long y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
         if (lane == 31) warp_sums[warp] = x;
         __syncthreads();
         if (warp == 0) {
-            int w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+            long long w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, w, o);
+                const long long y = __shfl_up_sync(0xffffffffu, w, o);
                 if (lane >= o) w += y;
             }
             warp_sums[lane] = w;
         }
         __syncthreads();
-        const int warp_prefix = warp ? warp_sums[warp - 1] : 0;
-        if (i < E) offs[i] = carry + warp_prefix + x - v;
+        const long long warp_prefix = warp ? warp_sums[warp - 1] : 0;
+        if (i < E) offs[i] = (int)min(carry + warp_prefix + x - v, 2147483647ll);
         __syncthreads();
         if (threadIdx.x == blockDim.x - 1) carry += warp_prefix + x;
         __syncthreads();
     }
-    if (threadIdx.x == 0) offs[E] = carry;
+    if (threadIdx.x == 0) offs[E] = (int)min(carry, 2147483647ll);
 }
 
 // ------------------------------------------------------------------ 3. FK
