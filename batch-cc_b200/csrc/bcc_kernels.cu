@@ -514,3 +514,189 @@ int robot_num_env_groups(int robot) { return robot == 0 ? PandaModel::num_env_gr
 int robot_dof(int robot) { return robot == 0 ? PandaModel::dof : -1; }
 
 }  // namespace bcc
+
+// ======================================================================
+// Records variant of the environment check (used by the allocation-free entry
+// point): works from the host-packed rounded-box records of bcc_pack_envs
+// (no interval-mask tables) and culls (primitive, link) pairs with an exact
+// AABB overlap test, one primitive per lane.  The walk over (sample, pair)
+// items is the same as check_kernel's.
+// ======================================================================
+namespace bcc {
+
+template <class M, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) check_records_kernel(RecordsParams P) {
+    constexpr int G = M::num_env_groups;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    __shared__ float4 boxes[WARPS][G][2];
+
+    const int env = blockIdx.x;
+    const int e_begin = blockIdx.y * P.edges_per_cta;
+    const int e_end = min(e_begin + P.edges_per_cta, P.num_edges);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p_begin = P.env_off[env];
+    const int np = P.env_off[env + 1] - p_begin;
+
+    const float4* prim = reinterpret_cast<const float4*>(smem);
+    uint16_t* pairs = reinterpret_cast<uint16_t*>(smem + (size_t)P.max_prims * kPrimF4 * 16) +
+                      (size_t)warp * P.pairs_per_warp;
+    if (np < 0 || np > P.max_prims) {  // shared memory was sized from the caller's max_prims
+        if (threadIdx.x == 0) atomicOr(P.error_flag, 2);
+        return;
+    }
+    if (np > 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            bulk_copy_g2s(smem, P.records + (size_t)p_begin * kPrimF4, (uint32_t)np * kPrimF4 * 16u, &bar);
+        if (!mbar_wait_bounded(&bar, 0u, 1u << 22)) {
+            if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
+            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
+            return;
+        }
+    }
+    const DevTables<M>& T = tab<M>();
+    const uint32_t lt = (1u << lane) - 1u;
+
+    for (int e = e_begin + warp; e < e_end; e += WARPS) {
+        uint8_t* out = P.results + (size_t)e * P.num_envs + env;
+        const int self = P.edge_self[e];
+        if (np == 0 || self) {
+            if (lane == 0) *out = self ? 1 : 0;
+            continue;
+        }
+        if (lane < G) {
+            boxes[warp][lane][0] = P.swept[((size_t)e * G + lane) * 2 + 0];
+            boxes[warp][lane][1] = P.swept[((size_t)e * G + lane) * 2 + 1];
+        }
+        __syncwarp();
+        // Exact AABB cull, one primitive per lane; pairs compacted link-major
+        // within each block of 32 primitives.
+        int C = 0;
+        for (int p0 = 0; p0 < np; p0 += 32) {
+            const int p = p0 + lane;
+            uint32_t mask = 0;
+            if (p < np) {
+                const float4 c = prim[p * kPrimF4 + 0];
+                const float4 h = prim[p * kPrimF4 + 4];
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    const float4 lo = boxes[warp][g][0], hi = boxes[warp][g][1];
+                    const bool ov = c.x - h.x <= hi.x && c.x + h.x >= lo.x && c.y - h.y <= hi.y &&
+                                    c.y + h.y >= lo.y && c.z - h.z <= hi.z && c.z + h.z >= lo.z;
+                    mask |= (uint32_t)ov << g;
+                }
+            }
+#pragma unroll 1
+            for (int g = 0; g < G; ++g) {
+                const uint32_t bits = __ballot_sync(0xffffffffu, (mask >> g) & 1u);
+                if ((mask >> g) & 1u) pairs[C + __popc(bits & lt)] = (uint16_t)((p << 4) | g);
+                C += __popc(bits);
+            }
+        }
+        __syncwarp();
+
+        bool collide = false;
+        if (C > 0) {
+            const int n = P.steps[e];
+            const int total = kLanes * n * C;
+            const size_t row0 = (size_t)P.offs[e];
+            const int dr = 32 / C, dc = 32 % C;
+            int r = lane / C, c = lane - (lane / C) * C;
+            for (int w0 = 0; w0 < total; w0 += 32) {
+                bool gate = false;
+                int g = 0, p = 0, k = 0;
+                if (w0 + lane < total) {
+                    k = reference_rank_to_sample(r, n);
+                    const uint32_t pr = pairs[c];
+                    g = (int)(pr & 15u);
+                    p = (int)(pr >> 4);
+                    float4 bs = P.table[(row0 + (size_t)k) * M::num_spheres + g];
+                    bs.w += kEnvInflate;
+                    gate = sphere_hits_prim(bs, prim + p * kPrimF4);
+                }
+                if (__any_sync(0xffffffffu, gate)) {
+                    const int cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
+                    int incl = cnt;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += y;
+                    }
+                    const int L = __shfl_sync(0xffffffffu, incl, 31);
+                    const int first = T.leaf_begin[g];
+                    for (int t0 = 0; t0 < L; t0 += 32) {
+                        const int t = t0 + lane;
+                        int j = 0;
+#pragma unroll
+                        for (int step = 16; step; step >>= 1) {
+                            const int v = __shfl_sync(0xffffffffu, incl, j + step - 1);
+                            if (v <= t) j += step;
+                        }
+                        const int j_incl = __shfl_sync(0xffffffffu, incl, j);
+                        const int j_cnt = __shfl_sync(0xffffffffu, cnt, j);
+                        const int j_first = __shfl_sync(0xffffffffu, first, j);
+                        const int j_k = __shfl_sync(0xffffffffu, k, j);
+                        const int j_p = __shfl_sync(0xffffffffu, p, j);
+                        bool hit = false;
+                        if (t < L) {
+                            const int leaf = j_first + (t - (j_incl - j_cnt));
+                            float4 ls = P.table[(row0 + (size_t)j_k) * M::num_spheres + G + leaf];
+                            ls.w += kEnvInflate;
+                            hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
+                        }
+                        if (__any_sync(0xffffffffu, hit)) {
+                            collide = true;
+                            break;
+                        }
+                    }
+                    if (collide) break;
+                }
+                c += dc;
+                r += dr;
+                if (c >= C) {
+                    c -= C;
+                    ++r;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) *out = collide ? 1 : 0;
+    }
+}
+
+size_t records_smem_bytes(int max_prims, int warps) {
+    const size_t ppw = (size_t)((max_prims * 16 + 7) & ~7);
+    return (size_t)max_prims * kPrimF4 * 16 + (size_t)warps * ppw * sizeof(uint16_t);
+}
+
+cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st) {
+    if (robot != 0) return cudaErrorInvalidValue;
+    using M = PandaModel;
+    const int E = a.num_edges;
+    const int R = a.total_rows;
+    if (R > 0) fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
+    if (R > 0) self_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
+    swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_records(int robot, RecordsParams P, cudaStream_t st) {
+    if (robot != 0) return cudaErrorInvalidValue;
+    using M = PandaModel;
+    constexpr int W = 4;
+    P.pairs_per_warp = (P.max_prims * 16 + 7) & ~7;
+    const size_t smem = records_smem_bytes(P.max_prims, W);
+    cudaError_t err = cudaFuncSetAttribute(check_records_kernel<M, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+    if (err != cudaSuccess) return err;
+    dim3 grid(P.num_envs, (P.num_edges + P.edges_per_cta - 1) / P.edges_per_cta);
+    check_records_kernel<M, W><<<grid, W * 32, smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace bcc

@@ -66,7 +66,30 @@ struct PipelineArgs {
     unsigned long long* counters;
 };
 
+// Environment check from host-packed records (bcc_pack_envs format), exact
+// AABB cull; used by the allocation-free entry point.
+struct RecordsParams {
+    const float4* records;   // [total prims][5] rounded-box records
+    const int* env_off;      // [num_envs + 1]
+    int num_envs;
+    int num_edges;
+    int max_prims;
+    int pairs_per_warp;
+    int edges_per_cta;
+    const int* steps;
+    const int* offs;
+    const float4* table;
+    const float4* swept;
+    const int* edge_self;
+    uint8_t* results;
+    int* error_flag;
+};
+
 cudaError_t upload_robot_tables(int robot);
+// FK table, self-collision and swept volumes only (no environment check).
+cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st);
+cudaError_t launch_check_records(int robot, RecordsParams P, cudaStream_t st);
+size_t records_smem_bytes(int max_prims, int warps);
 // Stage 1: steps + sample offsets (total rows land in offs[E]).
 cudaError_t launch_steps(int robot, const PipelineArgs& a, cudaStream_t st);
 // Stage 2: FK table, self-collision, swept volumes, environment check.

@@ -151,6 +151,30 @@ int32_t bcc_stage_times(bcc_ctx* ctx, float* ms, int32_t max_stages);
  */
 int32_t bcc_work_counters(bcc_ctx* ctx, uint64_t* out, int32_t max_counters);
 
+/*
+ * Allocation-free check.  No counterpart in the reference: this entry point
+ * exists for callers that cannot allocate device memory -- for example a
+ * planner checking edges from a real-time control thread, where cudaMalloc's
+ * implicit device synchronisation and unbounded latency are not allowed, or a
+ * host framework that owns all device memory through its own pool.  It makes
+ * no cudaMalloc/cudaFree or other allocating call and needs no bcc_ctx; its
+ * working buffers are fixed arrays inside the library (about 5 MB on every GPU
+ * that loads it, kept until the process exits).
+ *   d_records / d_env_offsets: device copies of bcc_pack_envs' output
+ *     (records 16-byte aligned); max_prims_per_env: its max_prims_per_env.
+ *   d_edges: device float[num_edges][2][dof]; d_results: device
+ *     uint8[num_edges][num_envs], same meaning and layout as bcc_check.
+ * Limits: num_edges <= 1024 and at most 4096 discretised samples per call
+ * (sum over edges of 32 n); beyond either the call returns BCC_ERR_LIMIT
+ * without checking anything.  Synchronous on `stream`.  The first call on a
+ * device sets that device up (resolves the arrays' addresses, uploads the robot
+ * tables): make it before any stream capture.  Every call reuses the same
+ * arrays, so calls that overlap on the GPU race; issue them one at a time.
+ */
+bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records, const int32_t* d_env_offsets,
+                             int32_t num_envs, int32_t max_prims_per_env, const float* d_edges,
+                             int32_t num_edges, int32_t resolution, uint8_t* d_results, void* stream);
+
 /* Diagnostics: FP32 FMA-pipe throughput of `device` in TFLOP/s, measured by a
  * short probe kernel (the roofline denominator of the scalar-FP32 checker). */
 bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
