@@ -60,6 +60,10 @@ def lib():
                                        ctypes.c_int32, ctypes.c_int32]
         L.bcc_robot_dof.argtypes = [ctypes.c_int]
         L.bcc_measure_fp32_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
+        L.bcc_mlp_num_params.argtypes = []
+        L.bcc_mlp_set_params.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
+        L.bcc_mlp_get_params.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
+        L.bcc_mlp_forward.argtypes = [vp, vp, ctypes.c_int32, vp, vp]
         L.bcc_set_profiling.argtypes = [vp, ctypes.c_int32]
         L.bcc_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]
         L.bcc_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
@@ -146,6 +150,21 @@ class Checker:
         if n < 0:
             raise BccError(1, "profiling is off or no check has run")
         return dict(zip(self.STAGES, [float(ms[i]) for i in range(n)]))
+
+    # ---------------------------------------------------------------- MLP
+    def mlp_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        self._raise(lib().bcc_mlp_set_params(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(p)))
+
+    def mlp_get_params(self):
+        n = lib().bcc_mlp_num_params()
+        p = np.zeros(n, np.float32)
+        self._raise(lib().bcc_mlp_get_params(self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n))
+        return p
+
+    def mlp_forward_device(self, d_x_ptr, rows, d_logits_ptr, stream=0):
+        self._raise(lib().bcc_mlp_forward(self._h, ctypes.c_void_p(d_x_ptr), rows, ctypes.c_void_p(d_logits_ptr),
+                                          ctypes.c_void_p(stream)))
 
     def check_device(self, d_edges_ptr, num_edges, d_results_ptr, resolution=32, robot="panda",
                      order="plain", stream=0, tile=0):

@@ -52,8 +52,16 @@ WORKLOADS = {
     "multi_baxter": dict(robot="baxter", envs=500, edges=5000, prims=(16, 256), edge_law="loglen",
                          box=(1.2, 1.2, 0.0, 1.8), density=1.0),
     "stress": dict(robot="panda", envs=10000, edges=100000, prims=(8, 128), edge_law="loglen",
-                   box=(0.8, 0.8, 0.0, 1.2), density=1.0),
+                   box=(0.8, 0.8, 0.0, 1.2), density=0.1, shell=True),
 }
+
+# Stress workload obstacle placement: a fraction `density` of obstacle centres
+# lies in the arm's reachable shell (distance 0.45-0.85 m from the shoulder,
+# above the floor), the rest beyond reach (1.05-1.6 m).  `density` is the
+# concentration multiplier tuned for a ~40 % colliding-edge fraction.
+SHOULDER = np.array([0.0, 0.0, 0.333])
+SHELL = (0.45, 0.85)
+OUTER = (1.05, 1.6)
 
 
 def euler_xyz_matrix(rho, theta, phi):
@@ -126,13 +134,16 @@ def gen_envs(name, num_envs=None, seed=0, density=None):
             nb, ns, nc = int((kind == 0).sum()), int((kind == 1).sum()), int((kind == 2).sum())
 
         def centres(m):
-            c = np.stack([rng.uniform(-bx, bx, m), rng.uniform(-by, by, m), rng.uniform(z0, z1, m)], -1)
-            if dens != 1.0:
-                # Pull centres toward the arm's reachable shell (radius ~0.6 m about
-                # (0, 0, 0.35)): density > 1 concentrates obstacles near the robot.
-                hub = np.array([0.0, 0.0, 0.35])
-                d = c - hub
-                c = hub + d / dens ** (1.0 / 3.0)
+            if not w.get("shell"):
+                return np.stack([rng.uniform(-bx, bx, m), rng.uniform(-by, by, m), rng.uniform(z0, z1, m)], -1)
+            d = rng.normal(size=(m, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            d[:, 2] = np.abs(d[:, 2]) * 0.8 - 0.2  # mostly above the shoulder plane
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            inner = rng.uniform(0, 1, m) < dens
+            rad = np.where(inner, rng.uniform(*SHELL, m), rng.uniform(*OUTER, m))
+            c = SHOULDER + d * rad[:, None]
+            c[:, 2] = np.maximum(c[:, 2], 0.0)
             return c
         sph = make_spheres(centres(ns), rng.uniform(0.05, 0.15, ns))
         yaw = rng.uniform(-math.pi, math.pi, nb)

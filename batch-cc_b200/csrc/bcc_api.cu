@@ -20,48 +20,7 @@
 #include "bcc_device.cuh"
 #include "bcc_kernels.h"
 
-namespace {
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    cudaError_t ensure(size_t bytes) {
-        if (bytes <= cap) return cudaSuccess;
-        const size_t want = std::max(bytes, cap * 3 / 2);
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e == cudaSuccess) cap = want;
-        return e;
-    }
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-};
-
-}  // namespace
-
-struct bcc_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    bool tables[3] = {false, false, false};
-    // environment arena
-    int num_envs = -1;
-    int max_prims = 0;
-    size_t blob_smem = 0;
-    DevBuf blobs, env_hdr;
-    // per-call buffers
-    DevBuf edges, steps, offs, table, row_edge, edge_self, swept, results, error_flag;
-    int* h_total = nullptr;  // pinned readback of the sample-row total
-    bool profiling = false;
-    bool counting = false;
-    DevBuf counters;
-    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-};
+#include "bcc_ctx.h"
 
 namespace {
 

@@ -1,0 +1,270 @@
+// bcc_mlp.cu -- the collision-likelihood MLP on 5th-generation tensor cores.
+//
+// Network (per sample configuration in one environment):
+//     x (48 = 7 normalised joints + 32 environment code + 9 zero) -> 128 -> 128 -> 128 -> 1
+// ReLU between layers, logit output.  Weights and activations are BF16 in
+// shared memory (core-matrix images, see bcc_tc.cuh), products accumulate in
+// FP32 tensor memory via tcgen05.mma (M = 128 rows per tile, N = 128), the
+// epilogues (bias, ReLU, final 128-wide dot product) run in FP32 registers.
+//
+// Parameters (FP32 masters, flat, kMlpParams floats):
+//     W1 [48][128] (in x out), b1 [128], W2 [128][128], b2 [128],
+//     W3 [128][128], b3 [128], w4 [128], b4 [1]
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/bcc.h"
+#include "bcc_ctx.h"
+#include "bcc_device.cuh"
+#include "bcc_mlp.h"
+#include "bcc_tc.cuh"
+
+namespace bcc {
+
+// Offsets of the parameter blocks in the flat FP32 vector.
+constexpr int kOffW1 = 0;
+constexpr int kOffB1 = kOffW1 + kMlpIn * kMlpHidden;
+constexpr int kOffW2 = kOffB1 + kMlpHidden;
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
+constexpr int kOffW3 = kOffB2 + kMlpHidden;
+constexpr int kOffB3 = kOffW3 + kMlpHidden * kMlpHidden;
+constexpr int kOffW4 = kOffB3 + kMlpHidden;
+constexpr int kOffB4 = kOffW4 + kMlpHidden;
+static_assert(kOffB4 + 1 == kMlpParams, "parameter layout");
+
+// Shared-memory map of the forward kernel (bytes).
+constexpr uint32_t kImgW1 = kMlpHidden * kMlpIn * 2;       // 12288
+constexpr uint32_t kImgW = kMlpHidden * kMlpHidden * 2;    // 32768
+constexpr uint32_t kSmW1 = 0;
+constexpr uint32_t kSmW2 = kSmW1 + kImgW1;
+constexpr uint32_t kSmW3 = kSmW2 + kImgW;
+constexpr uint32_t kSmX = kSmW3 + kImgW;                   // X tile 128 x 48
+constexpr uint32_t kSmH = kSmX + kImgW1;                   // H tile 128 x 128
+constexpr uint32_t kSmVec = kSmH + kImgW;                  // b1 b2 b3 w4 (4 x 128 floats) + b4
+constexpr uint32_t kSmBar = kSmVec + 4 * kMlpHidden * 4 + 16;
+constexpr uint32_t kSmTmem = kSmBar + 8;
+constexpr uint32_t kFwdSmem = kSmTmem + 8;
+constexpr uint32_t kImagesBytes = kImgW1 + 2 * kImgW;       // W1T | W2T | W3T
+
+// ---------------------------------------------------------------- images
+// FP32 masters -> BF16 core-matrix images of W1^T [128][48], W2^T, W3^T.
+__global__ void mlp_pack_kernel(const float* __restrict__ params, uint8_t* __restrict__ images) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n1 = kMlpHidden * kMlpIn, n2 = kMlpHidden * kMlpHidden;
+    if (i < n1) {
+        const int out = i / kMlpIn, in = i % kMlpIn;
+        const float w = params[kOffW1 + in * kMlpHidden + out];
+        *reinterpret_cast<__nv_bfloat16*>(images + tc::cm_offset(out, in, kMlpIn)) = __float2bfloat16_rn(w);
+    } else if (i < n1 + 2 * n2) {
+        const int j = i - n1;
+        const int layer = j / n2, r = j % n2;
+        const int out = r / kMlpHidden, in = r % kMlpHidden;
+        const float w = params[(layer ? kOffW3 : kOffW2) + in * kMlpHidden + out];
+        *reinterpret_cast<__nv_bfloat16*>(images + kImgW1 + layer * kImgW + tc::cm_offset(out, in, kMlpHidden)) =
+            __float2bfloat16_rn(w);
+    }
+}
+
+// ---------------------------------------------------------------- forward
+// Bias + ReLU of one 128-column accumulator row (this thread's row), written as
+// BF16 into the H image; `taddr` = TMEM address of column 0 of this warp's lanes.
+__device__ __forceinline__ void epilogue_relu_to_smem(uint32_t taddr, const float* bias, uint8_t* himg, int row) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(taddr + c0, v);
+        tc::wait_ld();
+        uint32_t packed[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float a = fmaxf(v[2 * i] + bias[c0 + 2 * i], 0.0f);
+            const float b = fmaxf(v[2 * i + 1] + bias[c0 + 2 * i + 1], 0.0f);
+            __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+            packed[i] = *reinterpret_cast<uint32_t*>(&h);
+        }
+        *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0, kMlpHidden)) =
+            make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0 + 8, kMlpHidden)) =
+            make_uint4(packed[4], packed[5], packed[6], packed[7]);
+    }
+}
+
+// Persistent: each CTA (4 warps, one row per thread) loads the weights once and
+// runs 128-row tiles.  x: BF16 [rows][48] row-major; logits: FP32 [rows].
+__global__ void __launch_bounds__(128, 1)
+    mlp_forward_kernel(const uint16_t* __restrict__ x, int rows, const uint4* __restrict__ images,
+                       const float* __restrict__ params, float* __restrict__ logits, int* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int t = threadIdx.x, warp = t >> 5;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSmTmem);
+    float* vec = reinterpret_cast<float*>(sm + kSmVec);
+
+    for (uint32_t i = t; i < kImagesBytes / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
+    for (int i = t; i < kMlpHidden; i += blockDim.x) {
+        vec[i] = params[kOffB1 + i];
+        vec[kMlpHidden + i] = params[kOffB2 + i];
+        vec[2 * kMlpHidden + i] = params[kOffB3 + i];
+        vec[3 * kMlpHidden + i] = params[kOffW4 + i];
+    }
+    if (t == 0) {
+        vec[4 * kMlpHidden] = params[kOffB4];
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc(tmem_slot, 128);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+    const uint32_t idesc = tc::make_idesc_bf16(128, kMlpHidden, 0, 0);
+    const uint32_t sbase = tc::smem_addr(sm);
+    uint32_t phase = 0;
+    bool bad = false;
+
+    const int tiles = (rows + 127) / 128;
+    for (int tile = blockIdx.x; tile < tiles && !bad; tile += gridDim.x) {
+        const int row = tile * 128 + t;
+        // X tile: this thread's row, six 16-byte chunks of 8 features.
+        const uint4* src = reinterpret_cast<const uint4*>(x + (size_t)row * kMlpIn);
+#pragma unroll
+        for (int j = 0; j < kMlpIn / 8; ++j) {
+            const uint4 v = row < rows ? src[j] : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(sm + kSmX + tc::cm_offset(t, 8 * j, kMlpIn)) = v;
+        }
+        // Three layers: MMAs from one thread, epilogue from all.
+#pragma unroll 1
+        for (int layer = 0; layer < 3; ++layer) {
+            tc::fence_async_smem();
+            tc::fence_before();
+            __syncthreads();
+            if (t == 0) {
+                tc::fence_after();
+                const uint32_t a0 = sbase + (layer == 0 ? kSmX : kSmH);
+                const uint32_t b0 = sbase + (layer == 0 ? kSmW1 : layer == 1 ? kSmW2 : kSmW3);
+                const int K = layer == 0 ? kMlpIn : kMlpHidden;
+                const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+                for (int s = 0; s < K / 16; ++s)
+                    tc::mma_bf16(tmem, tc::make_desc(a0 + 256u * s, 128u, sbo), tc::make_desc(b0 + 256u * s, 128u, sbo),
+                                 idesc, s > 0 ? 1u : 0u);
+                tc::commit(bar);
+            }
+            const bool ok = mbar_wait_bounded(bar, phase, 1u << 22);
+            if (__syncthreads_or(!ok)) {  // CTA-uniform decision
+                bad = true;
+                break;
+            }
+            phase ^= 1u;
+            tc::fence_after();
+            if (layer < 2) {
+                epilogue_relu_to_smem(taddr, vec + layer * kMlpHidden, sm + kSmH, t);
+            } else {
+                float acc = vec[4 * kMlpHidden];
+#pragma unroll 1
+                for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+                    float v[16];
+                    tc::tmem_ld16(taddr + c0, v);
+                    tc::wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        acc = fmaf(fmaxf(v[i] + vec[2 * kMlpHidden + c0 + i], 0.0f), vec[3 * kMlpHidden + c0 + i], acc);
+                }
+                if (row < rows) logits[row] = acc;
+            }
+        }
+    }
+    if (bad && t == 0) atomicOr(err, 1);
+    if (bad) mbar_wait_bounded(bar, phase, 1u << 22);  // let in-flight MMAs finish before freeing TMEM
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0) tc::tmem_free(tmem, 128);
+}
+
+cudaError_t mlp_pack(const float* d_params, uint8_t* d_images, cudaStream_t st) {
+    const int n = kMlpHidden * kMlpIn + 2 * kMlpHidden * kMlpHidden;
+    mlp_pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_params, d_images);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_forward(const uint16_t* d_x, int rows, const uint8_t* d_images, const float* d_params,
+                        float* d_logits, int* d_err, int num_sms, cudaStream_t st) {
+    if (rows <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+    if (e != cudaSuccess) return e;
+    const int tiles = (rows + 127) / 128;
+    const int grid = tiles < num_sms ? tiles : num_sms;
+    mlp_forward_kernel<<<grid, 128, kFwdSmem, st>>>(d_x, rows, reinterpret_cast<const uint4*>(d_images), d_params,
+                                                     d_logits, d_err);
+    return cudaGetLastError();
+}
+
+}  // namespace bcc
+
+// ====================================================================== C ABI
+namespace {
+
+bcc_status mlp_fail(bcc_ctx* c, bcc_status s, const char* msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+int sm_count(int dev) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bcc_mlp_num_params(void) { return bcc::kMlpParams; }
+
+bcc_status bcc_mlp_set_params(bcc_ctx* ctx, const float* params, int32_t n) {
+    if (!ctx || !params || n != bcc::kMlpParams) return mlp_fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad MLP parameters");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return BCC_ERR_CUDA;
+    bcc::MlpState& m = ctx->mlp;
+    const size_t pb = sizeof(float) * bcc::kMlpParams;
+    if (m.params.ensure(pb) != cudaSuccess || m.grads.ensure(pb) != cudaSuccess || m.adam_m.ensure(pb) != cudaSuccess ||
+        m.adam_v.ensure(pb) != cudaSuccess || m.images.ensure(bcc::kImagesBytes) != cudaSuccess)
+        return mlp_fail(ctx, BCC_ERR_CUDA, "MLP allocation failed");
+    if (cudaMemcpy(m.params.p, params, pb, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(m.adam_m.p, 0, pb) != cudaSuccess || cudaMemset(m.adam_v.p, 0, pb) != cudaSuccess)
+        return mlp_fail(ctx, BCC_ERR_CUDA, "MLP upload failed");
+    if (bcc::mlp_pack(m.params.as<float>(), m.images.as<uint8_t>(), ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return mlp_fail(ctx, BCC_ERR_CUDA, "MLP pack failed");
+    m.step = 0;
+    m.ready = true;
+    return BCC_OK;
+}
+
+bcc_status bcc_mlp_get_params(bcc_ctx* ctx, float* params, int32_t n) {
+    if (!ctx || !params || n != bcc::kMlpParams || !ctx->mlp.ready) return BCC_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess ||
+        cudaMemcpy(params, ctx->mlp.params.p, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return BCC_ERR_CUDA;
+    return BCC_OK;
+}
+
+bcc_status bcc_mlp_forward(bcc_ctx* ctx, const void* d_x_bf16, int32_t rows, float* d_logits, void* stream) {
+    if (!ctx || !ctx->mlp.ready) return mlp_fail(ctx, BCC_ERR_INVALID_ARGUMENT, "MLP parameters not set");
+    if (rows < 0 || (rows > 0 && (!d_x_bf16 || !d_logits))) return mlp_fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad MLP input");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return BCC_ERR_CUDA;
+    if (ctx->error_flag.ensure(sizeof(int)) != cudaSuccess) return BCC_ERR_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(ctx->error_flag.p, 0, sizeof(int), st) != cudaSuccess) return BCC_ERR_CUDA;
+    if (bcc::mlp_forward(static_cast<const uint16_t*>(d_x_bf16), rows, ctx->mlp.images.as<uint8_t>(),
+                         ctx->mlp.params.as<float>(), d_logits, ctx->error_flag.as<int>(), sm_count(ctx->device),
+                         st) != cudaSuccess)
+        return mlp_fail(ctx, BCC_ERR_CUDA, "MLP forward launch failed");
+    return BCC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,20 @@
+// bcc_mlp.h -- shapes and launchers of the collision-likelihood MLP (internal).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bcc {
+
+constexpr int kMlpIn = 48;       // 7 joints + 32 environment code + 9 zero padding
+constexpr int kMlpJoints = 7;
+constexpr int kEnvCode = 32;
+constexpr int kMlpHidden = 128;
+constexpr int kMlpParams = kMlpIn * kMlpHidden + kMlpHidden + 2 * (kMlpHidden * kMlpHidden + kMlpHidden) +
+                           kMlpHidden + 1;
+
+cudaError_t mlp_pack(const float* d_params, uint8_t* d_images, cudaStream_t st);
+cudaError_t mlp_forward(const uint16_t* d_x, int rows, const uint8_t* d_images, const float* d_params,
+                        float* d_logits, int* d_err, int num_sms, cudaStream_t st);
+
+}  // namespace bcc

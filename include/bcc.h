@@ -175,6 +175,22 @@ bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records, const int3
                              int32_t num_envs, int32_t max_prims_per_env, const float* d_edges,
                              int32_t num_edges, int32_t resolution, uint8_t* d_results, void* stream);
 
+/*
+ * Collision-likelihood MLP of the learned check order (no reference
+ * counterpart; the north-star learned proposal).  Input row: 48 BF16 features
+ * (7 joints normalised to [-1, 1] by the joint limits, 32-value environment
+ * code, 9 zeros); 3 hidden layers of 128 (ReLU); output: one logit
+ * (collision likelihood).  Parameters are FP32 masters, flat, in the order
+ * W1[48][128], b1[128], W2[128][128], b2[128], W3[128][128], b3[128], w4[128],
+ * b4[1]; the kernels use BF16 copies on tcgen05 tensor cores with FP32
+ * accumulation.
+ */
+int32_t bcc_mlp_num_params(void);
+bcc_status bcc_mlp_set_params(bcc_ctx* ctx, const float* params, int32_t num_params);
+bcc_status bcc_mlp_get_params(bcc_ctx* ctx, float* params, int32_t num_params);
+/* d_x: device BF16 [rows][48]; d_logits: device FP32 [rows]; stream-ordered. */
+bcc_status bcc_mlp_forward(bcc_ctx* ctx, const void* d_x_bf16, int32_t rows, float* d_logits, void* stream);
+
 /* Diagnostics: FP32 FMA-pipe throughput of `device` in TFLOP/s, measured by a
  * short probe kernel (the roofline denominator of the scalar-FP32 checker). */
 bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
