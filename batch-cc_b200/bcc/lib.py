@@ -64,6 +64,9 @@ def lib():
         L.bcc_mlp_set_params.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
         L.bcc_mlp_get_params.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
         L.bcc_mlp_forward.argtypes = [vp, vp, ctypes.c_int32, vp, vp]
+        L.bcc_mlp_gradients.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_float),
+                                        ctypes.POINTER(ctypes.c_float)]
+        L.bcc_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
         L.bcc_set_profiling.argtypes = [vp, ctypes.c_int32]
         L.bcc_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]
         L.bcc_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
@@ -165,6 +168,20 @@ class Checker:
     def mlp_forward_device(self, d_x_ptr, rows, d_logits_ptr, stream=0):
         self._raise(lib().bcc_mlp_forward(self._h, ctypes.c_void_p(d_x_ptr), rows, ctypes.c_void_p(d_logits_ptr),
                                           ctypes.c_void_p(stream)))
+
+    def mlp_gradients_device(self, d_x_ptr, d_y_ptr, rows):
+        n = lib().bcc_mlp_num_params()
+        g = np.zeros(n, np.float32)
+        loss = ctypes.c_float(0)
+        self._raise(lib().bcc_mlp_gradients(self._h, ctypes.c_void_p(d_x_ptr), ctypes.c_void_p(d_y_ptr), rows,
+                                            g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(loss)))
+        return g, float(loss.value)
+
+    def mlp_train_step_device(self, d_x_ptr, d_y_ptr, rows, lr):
+        loss = ctypes.c_float(0)
+        self._raise(lib().bcc_mlp_train_step(self._h, ctypes.c_void_p(d_x_ptr), ctypes.c_void_p(d_y_ptr), rows,
+                                             ctypes.c_float(lr), ctypes.byref(loss)))
+        return float(loss.value)
 
     def check_device(self, d_edges_ptr, num_edges, d_results_ptr, resolution=32, robot="panda",
                      order="plain", stream=0, tile=0):

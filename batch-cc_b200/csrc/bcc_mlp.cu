@@ -186,6 +186,314 @@ __global__ void __launch_bounds__(128, 1)
     if (warp == 0) tc::tmem_free(tmem, 128);
 }
 
+// ---------------------------------------------------------------- training
+// One CTA (128 threads, one row per thread) runs forward and backward over its
+// 128-row tiles.  Activations stay in shared memory as BF16 images; the three
+// weight-gradient accumulators stay in tensor memory across tiles and are
+// added to the global FP32 gradient once at the end.  Loss: mean binary
+// cross-entropy of the logit against the 0/1 label (scale = 1 / total rows).
+//
+// GEMMs (M = 128 unless noted; "K" / "MN" = operand read K- or MN-major):
+//   forward   z1 = X W1 (A=X K, B=W1T K), z2 = H1 W2, z3 = H2 W3
+//   backward  dW3 += H2^T dZ3   (A=H2 MN, B=dZ3 MN, K = rows)
+//             dH2  = dZ3 W3^T   (A=dZ3 K, B=W3T MN)
+//             dW2 += H1^T dZ2,  dH1 = dZ2 W2^T
+//             dW1^T += dZ1^T X  (A=dZ1 MN, B=X MN, N = 48)
+constexpr uint32_t kTrW1 = 0;
+constexpr uint32_t kTrW2 = kTrW1 + kImgW1;
+constexpr uint32_t kTrW3 = kTrW2 + kImgW;
+constexpr uint32_t kTrX = kTrW3 + kImgW;
+constexpr uint32_t kTrH1 = kTrX + kImgW1;
+constexpr uint32_t kTrH2 = kTrH1 + kImgW;
+constexpr uint32_t kTrD = kTrH2 + kImgW;
+constexpr uint32_t kTrVec = kTrD + kImgW;                 // b1 b2 b3 w4 b4 (params)
+constexpr uint32_t kTrGrad = kTrVec + 5 * kMlpHidden * 4;  // db1 db2 db3 dw4 db4 loss
+constexpr uint32_t kTrBar = kTrGrad + 5 * kMlpHidden * 4 + 16;
+constexpr uint32_t kTrTmem = kTrBar + 8;
+constexpr uint32_t kTrainSmem = kTrTmem + 8;
+// TMEM columns: forward / backward-data accumulator, dW3, dW2, dW1^T.
+constexpr uint32_t kColAcc = 0, kColW3 = 128, kColW2 = 256, kColW1 = 384;
+
+__device__ __forceinline__ void gemm_issue(uint32_t d, uint32_t a0, uint32_t a_lbo, uint32_t a_sbo, uint32_t a_step,
+                                           uint32_t b0, uint32_t b_lbo, uint32_t b_sbo, uint32_t b_step, int ksteps,
+                                           uint32_t idesc, bool accumulate) {
+    for (int s = 0; s < ksteps; ++s)
+        tc::mma_bf16(d, tc::make_desc(a0 + a_step * s, a_lbo, a_sbo), tc::make_desc(b0 + b_step * s, b_lbo, b_sbo),
+                     idesc, (accumulate || s > 0) ? 1u : 0u);
+}
+
+// Column sums over the CTA's 128 rows of per-row values v[0..15] (columns
+// c0..c0+15), added into acc[c0 + i] in shared memory.
+__device__ __forceinline__ void colsum16(const float* v, float* acc, int c0) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        float x = v[i];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == i) atomicAdd(acc + c0 + i, x);
+    }
+}
+
+__device__ __forceinline__ float bf16_at(const uint8_t* img, int r, int c, int K) {
+    return __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(img + tc::cm_offset(r, c, K)));
+}
+
+__global__ void __launch_bounds__(128, 1)
+    mlp_train_kernel(const uint16_t* __restrict__ x, const uint8_t* __restrict__ y, int rows,
+                     const uint4* __restrict__ images, const float* __restrict__ params, float* __restrict__ grads,
+                     float* __restrict__ loss_sum, int* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int t = threadIdx.x, warp = t >> 5;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTrBar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kTrTmem);
+    float* vec = reinterpret_cast<float*>(sm + kTrVec);    // b1 | b2 | b3 | w4 | b4
+    float* gv = reinterpret_cast<float*>(sm + kTrGrad);    // db1 | db2 | db3 | dw4 | db4, loss
+    const float inv_rows = 1.0f / (float)rows;
+
+    for (uint32_t i = t; i < kImagesBytes / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
+    for (int i = t; i < kMlpHidden; i += blockDim.x) {
+        vec[i] = params[kOffB1 + i];
+        vec[kMlpHidden + i] = params[kOffB2 + i];
+        vec[2 * kMlpHidden + i] = params[kOffB3 + i];
+        vec[3 * kMlpHidden + i] = params[kOffW4 + i];
+    }
+    for (int i = t; i < 5 * kMlpHidden + 4; i += blockDim.x) gv[i] = 0.0f;
+    if (t == 0) {
+        vec[4 * kMlpHidden] = params[kOffB4];
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) tc::tmem_alloc(tmem_slot, 512);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
+    const uint32_t sb = tc::smem_addr(sm);
+    const uint32_t id_fwd = tc::make_idesc_bf16(128, 128, 0, 0);   // A K-major, B K-major
+    const uint32_t id_dw = tc::make_idesc_bf16(128, 128, 1, 1);    // A MN, B MN
+    const uint32_t id_dh = tc::make_idesc_bf16(128, 128, 0, 1);    // A K, B MN
+    const uint32_t id_dw1 = tc::make_idesc_bf16(128, 48, 1, 1);    // dW1^T: N = 48
+    uint32_t phase = 0;
+    bool bad = false, first = true;
+    float* db1 = gv;
+    float* db2 = gv + kMlpHidden;
+    float* db3 = gv + 2 * kMlpHidden;
+    float* dw4 = gv + 3 * kMlpHidden;
+
+    // Issue (thread 0) + wait (all): returns false on a timed-out wait.
+    auto sync_issue = [&](auto&& issue) -> bool {
+        tc::fence_async_smem();
+        tc::fence_before();
+        __syncthreads();
+        if (t == 0) {
+            tc::fence_after();
+            issue();
+            tc::commit(bar);
+        }
+        const bool ok = mbar_wait_bounded(bar, phase, 1u << 22);
+        if (__syncthreads_or(!ok)) return false;
+        phase ^= 1u;
+        tc::fence_after();
+        return true;
+    };
+
+    const int tiles = (rows + 127) / 128;
+    for (int tile = blockIdx.x; tile < tiles && !bad; tile += gridDim.x) {
+        const int row = tile * 128 + t;
+        const bool live = row < rows;
+        const uint4* src = reinterpret_cast<const uint4*>(x + (size_t)row * kMlpIn);
+#pragma unroll
+        for (int j = 0; j < kMlpIn / 8; ++j)
+            *reinterpret_cast<uint4*>(sm + kTrX + tc::cm_offset(t, 8 * j, kMlpIn)) = live ? src[j] : make_uint4(0, 0, 0, 0);
+        const float label = live ? (float)y[row] : 0.0f;
+
+        // ---- forward
+        if (!sync_issue([&] { gemm_issue(tmem + kColAcc, sb + kTrX, 128, 768, 256, sb + kTrW1, 128, 768, 256, 3, id_fwd, false); })) { bad = true; break; }
+        epilogue_relu_to_smem(tmem + lane_off + kColAcc, vec, sm + kTrH1, t);
+        if (!sync_issue([&] { gemm_issue(tmem + kColAcc, sb + kTrH1, 128, 2048, 256, sb + kTrW2, 128, 2048, 256, 8, id_fwd, false); })) { bad = true; break; }
+        epilogue_relu_to_smem(tmem + lane_off + kColAcc, vec + kMlpHidden, sm + kTrH2, t);
+        if (!sync_issue([&] { gemm_issue(tmem + kColAcc, sb + kTrH2, 128, 2048, 256, sb + kTrW3, 128, 2048, 256, 8, id_fwd, false); })) { bad = true; break; }
+        float logit = vec[4 * kMlpHidden];
+#pragma unroll 1
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + lane_off + kColAcc + c0, v);
+            tc::wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) logit = fmaf(fmaxf(v[i] + vec[2 * kMlpHidden + c0 + i], 0.0f), vec[3 * kMlpHidden + c0 + i], logit);
+        }
+        // ---- loss and dlogit (mean BCE)
+        const float prob = 1.0f / (1.0f + __expf(-logit));
+        const float dlogit = live ? (prob - label) * inv_rows : 0.0f;
+        const float l = live ? (fmaxf(logit, 0.0f) - logit * label + log1pf(__expf(-fabsf(logit)))) : 0.0f;
+        {
+            float s1 = l, s2 = dlogit;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            }
+            if ((t & 31) == 0) {
+                atomicAdd(gv + 5 * kMlpHidden + 1, s1);
+                atomicAdd(gv + 4 * kMlpHidden, s2);
+            }
+        }
+        // dz3 = dlogit * w4 * (h3 > 0); dw4 += dlogit * h3; db3 += dz3
+#pragma unroll 1
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+            float v[16], g3[16], gw[16];
+            tc::tmem_ld16(tmem + lane_off + kColAcc + c0, v);
+            tc::wait_ld();
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const float h3 = fmaxf(v[i] + vec[2 * kMlpHidden + c0 + i], 0.0f);
+                gw[i] = dlogit * h3;
+                g3[i] = h3 > 0.0f ? dlogit * vec[3 * kMlpHidden + c0 + i] : 0.0f;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                __nv_bfloat162 h = __floats2bfloat162_rn(g3[2 * i], g3[2 * i + 1]);
+                packed[i] = *reinterpret_cast<uint32_t*>(&h);
+            }
+            *reinterpret_cast<uint4*>(sm + kTrD + tc::cm_offset(t, c0, kMlpHidden)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            *reinterpret_cast<uint4*>(sm + kTrD + tc::cm_offset(t, c0 + 8, kMlpHidden)) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+            colsum16(gw, dw4, c0);
+            colsum16(g3, db3, c0);
+        }
+        // ---- dW3 += H2^T dZ3 ; dH2 = dZ3 W3^T
+        const bool acc_w = !first;
+        if (!sync_issue([&] {
+                gemm_issue(tmem + kColW3, sb + kTrH2, 2048, 128, 4096, sb + kTrD, 2048, 128, 4096, 8, id_dw, acc_w);
+                gemm_issue(tmem + kColAcc, sb + kTrD, 128, 2048, 256, sb + kTrW3, 2048, 128, 4096, 8, id_dh, false);
+            })) { bad = true; break; }
+        // dz2 = dh2 * (h2 > 0) -> D ; db2 += dz2
+#pragma unroll 1
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + lane_off + kColAcc + c0, v);
+            tc::wait_ld();
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = bf16_at(sm + kTrH2, t, c0 + i, kMlpHidden) > 0.0f ? v[i] : 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                packed[i] = *reinterpret_cast<uint32_t*>(&h);
+            }
+            *reinterpret_cast<uint4*>(sm + kTrD + tc::cm_offset(t, c0, kMlpHidden)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            *reinterpret_cast<uint4*>(sm + kTrD + tc::cm_offset(t, c0 + 8, kMlpHidden)) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+            colsum16(v, db2, c0);
+        }
+        // ---- dW2 += H1^T dZ2 ; dH1 = dZ2 W2^T
+        if (!sync_issue([&] {
+                gemm_issue(tmem + kColW2, sb + kTrH1, 2048, 128, 4096, sb + kTrD, 2048, 128, 4096, 8, id_dw, acc_w);
+                gemm_issue(tmem + kColAcc, sb + kTrD, 128, 2048, 256, sb + kTrW2, 2048, 128, 4096, 8, id_dh, false);
+            })) { bad = true; break; }
+#pragma unroll 1
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + lane_off + kColAcc + c0, v);
+            tc::wait_ld();
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = bf16_at(sm + kTrH1, t, c0 + i, kMlpHidden) > 0.0f ? v[i] : 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                packed[i] = *reinterpret_cast<uint32_t*>(&h);
+            }
+            *reinterpret_cast<uint4*>(sm + kTrD + tc::cm_offset(t, c0, kMlpHidden)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            *reinterpret_cast<uint4*>(sm + kTrD + tc::cm_offset(t, c0 + 8, kMlpHidden)) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+            colsum16(v, db1, c0);
+        }
+        // ---- dW1^T += dZ1^T X
+        if (!sync_issue([&] {
+                gemm_issue(tmem + kColW1, sb + kTrD, 2048, 128, 4096, sb + kTrX, 768, 128, 1536, 8, id_dw1, acc_w);
+            })) { bad = true; break; }
+        first = false;
+    }
+    if (bad) {
+        if (t == 0) atomicOr(err, 1);
+        mbar_wait_bounded(bar, phase, 1u << 22);
+    }
+    // ---- write gradients: thread t owns TMEM lane t of each accumulator.
+    if (!bad && !first) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + lane_off + kColW3 + c0, v);
+            tc::wait_ld();
+            for (int i = 0; i < 16; ++i) atomicAdd(grads + kOffW3 + t * kMlpHidden + c0 + i, v[i]);
+            tc::tmem_ld16(tmem + lane_off + kColW2 + c0, v);
+            tc::wait_ld();
+            for (int i = 0; i < 16; ++i) atomicAdd(grads + kOffW2 + t * kMlpHidden + c0 + i, v[i]);
+        }
+#pragma unroll 1
+        for (int c0 = 0; c0 < kMlpIn; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + lane_off + kColW1 + c0, v);
+            tc::wait_ld();
+            for (int i = 0; i < 16; ++i) atomicAdd(grads + kOffW1 + (c0 + i) * kMlpHidden + t, v[i]);
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (!bad) {
+        atomicAdd(grads + kOffB1 + t, db1[t]);
+        atomicAdd(grads + kOffB2 + t, db2[t]);
+        atomicAdd(grads + kOffB3 + t, db3[t]);
+        atomicAdd(grads + kOffW4 + t, dw4[t]);
+        if (t == 0) {
+            atomicAdd(grads + kOffB4, gv[4 * kMlpHidden]);
+            atomicAdd(loss_sum, gv[5 * kMlpHidden + 1]);
+        }
+    }
+    if (warp == 0) tc::tmem_free(tmem, 512);
+}
+
+// Adam on the FP32 masters (bias-corrected), then the BF16 images are re-packed.
+__global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1,
+                                float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+cudaError_t mlp_train_grads(const uint16_t* d_x, const uint8_t* d_y, int rows, const uint8_t* d_images,
+                            const float* d_params, float* d_grads, float* d_loss, int* d_err, int num_sms,
+                            cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_grads, 0, sizeof(float) * kMlpParams, st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(d_loss, 0, sizeof(float), st);
+    if (e != cudaSuccess) return e;
+    if (rows <= 0) return cudaSuccess;
+    e = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem);
+    if (e != cudaSuccess) return e;
+    const int tiles = (rows + 127) / 128;
+    const int grid = tiles < num_sms ? tiles : num_sms;
+    mlp_train_kernel<<<grid, 128, kTrainSmem, st>>>(d_x, d_y, rows, reinterpret_cast<const uint4*>(d_images), d_params,
+                                                    d_grads, d_loss, d_err);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_adam(float* d_params, const float* d_grads, float* d_m, float* d_v, long long step, float lr,
+                     cudaStream_t st) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(d_params, d_grads, d_m, d_v, kMlpParams, lr, b1, b2,
+                                                              1e-8f, c1, c2);
+    return cudaGetLastError();
+}
+
 cudaError_t mlp_pack(const float* d_params, uint8_t* d_images, cudaStream_t st) {
     const int n = kMlpHidden * kMlpIn + 2 * kMlpHidden * kMlpHidden;
     mlp_pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_params, d_images);
@@ -264,6 +572,49 @@ bcc_status bcc_mlp_forward(bcc_ctx* ctx, const void* d_x_bf16, int32_t rows, flo
                          ctx->mlp.params.as<float>(), d_logits, ctx->error_flag.as<int>(), sm_count(ctx->device),
                          st) != cudaSuccess)
         return mlp_fail(ctx, BCC_ERR_CUDA, "MLP forward launch failed");
+    return BCC_OK;
+}
+
+// Gradients (and summed loss) of the mean BCE over `rows` labelled rows,
+// computed by the tensor-core training kernel; written to host arrays.
+bcc_status bcc_mlp_gradients(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows,
+                             float* h_grads, float* h_loss) {
+    if (!ctx || !ctx->mlp.ready) return mlp_fail(ctx, BCC_ERR_INVALID_ARGUMENT, "MLP parameters not set");
+    if (rows < 0 || (rows > 0 && (!d_x_bf16 || !d_labels))) return BCC_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return BCC_ERR_CUDA;
+    bcc::MlpState& m = ctx->mlp;
+    if (ctx->error_flag.ensure(sizeof(int)) != cudaSuccess || m.logits.ensure(sizeof(float) * 4) != cudaSuccess)
+        return BCC_ERR_CUDA;
+    cudaStream_t st = ctx->stream;
+    if (cudaMemsetAsync(ctx->error_flag.p, 0, sizeof(int), st) != cudaSuccess) return BCC_ERR_CUDA;
+    if (bcc::mlp_train_grads(static_cast<const uint16_t*>(d_x_bf16), d_labels, rows, m.images.as<uint8_t>(),
+                             m.params.as<float>(), m.grads.as<float>(), m.logits.as<float>(), ctx->error_flag.as<int>(),
+                             sm_count(ctx->device), st) != cudaSuccess)
+        return mlp_fail(ctx, BCC_ERR_CUDA, "MLP training kernel launch failed");
+    int flag = 0;
+    if (cudaMemcpyAsync(&flag, ctx->error_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return BCC_ERR_CUDA;
+    if (flag) return mlp_fail(ctx, BCC_ERR_TIMEOUT, "MLP training kernel wait timed out");
+    if (h_grads && cudaMemcpy(h_grads, m.grads.p, sizeof(float) * bcc::kMlpParams, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return BCC_ERR_CUDA;
+    if (h_loss && cudaMemcpy(h_loss, m.logits.p, sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return BCC_ERR_CUDA;
+    return BCC_OK;
+}
+
+// One optimisation step: gradients of the batch, Adam update (lr), re-pack.
+bcc_status bcc_mlp_train_step(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows, float lr,
+                              float* h_loss) {
+    bcc_status s = bcc_mlp_gradients(ctx, d_x_bf16, d_labels, rows, nullptr, h_loss);
+    if (s != BCC_OK) return s;
+    bcc::MlpState& m = ctx->mlp;
+    m.step += 1;
+    if (bcc::mlp_adam(m.params.as<float>(), m.grads.as<float>(), m.adam_m.as<float>(), m.adam_v.as<float>(), m.step, lr,
+                      ctx->stream) != cudaSuccess ||
+        bcc::mlp_pack(m.params.as<float>(), m.images.as<uint8_t>(), ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return mlp_fail(ctx, BCC_ERR_CUDA, "MLP update failed");
     return BCC_OK;
 }
 

@@ -17,4 +17,10 @@ cudaError_t mlp_pack(const float* d_params, uint8_t* d_images, cudaStream_t st);
 cudaError_t mlp_forward(const uint16_t* d_x, int rows, const uint8_t* d_images, const float* d_params,
                         float* d_logits, int* d_err, int num_sms, cudaStream_t st);
 
+cudaError_t mlp_train_grads(const uint16_t* d_x, const uint8_t* d_y, int rows, const uint8_t* d_images,
+                            const float* d_params, float* d_grads, float* d_loss, int* d_err, int num_sms,
+                            cudaStream_t st);
+cudaError_t mlp_adam(float* d_params, const float* d_grads, float* d_m, float* d_v, long long step, float lr,
+                     cudaStream_t st);
+
 }  // namespace bcc

@@ -190,6 +190,15 @@ bcc_status bcc_mlp_set_params(bcc_ctx* ctx, const float* params, int32_t num_par
 bcc_status bcc_mlp_get_params(bcc_ctx* ctx, float* params, int32_t num_params);
 /* d_x: device BF16 [rows][48]; d_logits: device FP32 [rows]; stream-ordered. */
 bcc_status bcc_mlp_forward(bcc_ctx* ctx, const void* d_x_bf16, int32_t rows, float* d_logits, void* stream);
+/* Gradient of the mean binary cross-entropy over `rows` labelled rows (labels
+ * 0/1, device uint8) with respect to every parameter, by the tensor-core
+ * training kernel; h_grads: host FP32 [num_params] (may be NULL), h_loss: host
+ * summed loss (may be NULL). */
+bcc_status bcc_mlp_gradients(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows,
+                             float* h_grads, float* h_loss);
+/* One Adam step (learning rate lr) on the gradient of the batch. */
+bcc_status bcc_mlp_train_step(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows,
+                              float lr, float* h_loss);
 
 /* Diagnostics: FP32 FMA-pipe throughput of `device` in TFLOP/s, measured by a
  * short probe kernel (the roofline denominator of the scalar-FP32 checker). */
