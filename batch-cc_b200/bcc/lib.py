@@ -67,6 +67,13 @@ def lib():
         L.bcc_mlp_gradients.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_float)]
         L.bcc_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
+        L.bcc_mlp_train.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_uint64,
+                                    ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+        L.bcc_mlp_evaluate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
+        L.bcc_last_learned_rows.argtypes = [vp]
+        L.bcc_last_learned_rows.restype = ctypes.c_int64
         L.bcc_set_profiling.argtypes = [vp, ctypes.c_int32]
         L.bcc_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]
         L.bcc_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
@@ -182,6 +189,28 @@ class Checker:
         self._raise(lib().bcc_mlp_train_step(self._h, ctypes.c_void_p(d_x_ptr), ctypes.c_void_p(d_y_ptr), rows,
                                              ctypes.c_float(lr), ctypes.byref(loss)))
         return float(loss.value)
+
+    def mlp_train(self, edges, num_samples, epochs=2, batch=16384, lr=2e-3, seed=0, resolution=32, robot="panda"):
+        """Train on checker-labelled samples of the uploaded envs; returns (epoch losses, positive fraction)."""
+        edges = np.ascontiguousarray(edges, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        pos = ctypes.c_float(0)
+        self._raise(lib().bcc_mlp_train(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                        len(edges), resolution, int(num_samples), epochs, batch, ctypes.c_float(lr),
+                                        ctypes.c_uint64(seed), losses.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                        ctypes.byref(pos)))
+        return losses, float(pos.value)
+
+    def mlp_evaluate(self, edges, num_samples, seed=1, resolution=32, robot="panda"):
+        edges = np.ascontiguousarray(edges, np.float32)
+        m = np.zeros(5, np.float32)
+        self._raise(lib().bcc_mlp_evaluate(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                           len(edges), resolution, int(num_samples), ctypes.c_uint64(seed),
+                                           m.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return dict(zip(("loss", "mispredict", "false_pos", "false_neg", "positive"), [float(v) for v in m]))
+
+    def last_learned_rows(self):
+        return int(lib().bcc_last_learned_rows(self._h))
 
     def check_device(self, d_edges_ptr, num_edges, d_results_ptr, resolution=32, robot="panda",
                      order="plain", stream=0, tile=0):

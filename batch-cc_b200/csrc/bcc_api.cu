@@ -19,6 +19,7 @@
 #include "../../include/bcc.h"
 #include "bcc_device.cuh"
 #include "bcc_kernels.h"
+#include "bcc_mlp.h"
 
 #include "bcc_ctx.h"
 
@@ -133,16 +134,17 @@ Rec rec_cuboid(const float* b, bool z_aligned) {
 
 int clamp_tile(int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); }
 
-bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution,
-                     uint8_t* d_results, const bcc_opts* opts, cudaStream_t st) {
+// Discretisation, sample offsets and every per-call buffer of a check; fills
+// `a` up to (not including) the FK / self / swept / check launches.
+bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution, uint8_t* d_results,
+                   const bcc_opts* opts, cudaStream_t st, bcc::PipelineArgs& a) {
     const int r = (int)robot;
     if (r != BCC_ROBOT_PANDA) return fail(ctx, BCC_ERR_NOT_SUPPORTED, "robot not built into this library");
     if (!ctx->tables[r]) {
         BCC_CUDA(ctx, bcc::upload_robot_tables(r));
         ctx->tables[r] = true;
     }
-    (void)opts;
-    bcc::PipelineArgs a{};
+    a = bcc::PipelineArgs{};
     a.d_edges = d_edges;
     a.num_edges = E;
     a.resolution = resolution;
@@ -193,7 +195,81 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     a.edges_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : 128, 1, 1 << 20);
     if ((E + a.edges_per_cta - 1) / a.edges_per_cta > 65535)
         a.edges_per_cta = (E + 65534) / 65535;
-    BCC_CUDA(ctx, bcc::launch_check(r, a, st));
+    return BCC_OK;
+}
+
+// Environment codes of the uploaded set (once per upload).
+bcc_status ensure_env_code(bcc_ctx* ctx, cudaStream_t st) {
+    if (ctx->env_code_ready) return BCC_OK;
+    BCC_CUDA(ctx, ctx->env_code.ensure(sizeof(float) * 32 * (size_t)std::max(ctx->num_envs, 1)));
+    BCC_CUDA(ctx, bcc::launch_env_encode(ctx->blobs.as<float4>(), ctx->env_hdr.as<float4>(), ctx->num_envs,
+                                         ctx->env_code.as<float>(), st));
+    ctx->env_code_ready = true;
+    return BCC_OK;
+}
+
+constexpr int kLearnedRowCap = 16 << 20;  // MLP rows per learned check (1.5 GB of features)
+
+// Learned order: (1) plain probe of each pair's first chunk, undecided pairs
+// queued with MLP rows for their segments; (2) segment features and tcgen05
+// MLP scores; (3) the queued pairs walked in descending segment score.
+bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
+    if (!ctx->mlp.ready) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned order needs MLP parameters (bcc_mlp_train or bcc_mlp_set_params)");
+    bcc_status s = ensure_env_code(ctx, st);
+    if (s != BCC_OK) return s;
+    const int grid = bcc::check_grid_size(a);
+    const size_t qn = (size_t)grid * a.edges_per_cta;
+    BCC_CUDA(ctx, ctx->q_count.ensure(sizeof(int) * (size_t)grid + 64));
+    BCC_CUDA(ctx, ctx->q_edges.ensure(sizeof(int) * qn));
+    BCC_CUDA(ctx, ctx->q_rows.ensure(sizeof(int) * qn));
+    long long cap_ll = (long long)a.num_envs * (a.total_rows / bcc::kSegment) + 64;
+    const int cap = (int)std::min<long long>(cap_ll, kLearnedRowCap);
+    BCC_CUDA(ctx, ctx->mlp.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)cap));
+    BCC_CUDA(ctx, ctx->mlp.logits.ensure(sizeof(float) * (size_t)cap));
+    a.q_count = ctx->q_count.as<int>();
+    a.row_count = a.q_count + grid;  // one counter past the per-CTA counts
+    a.q_edges = ctx->q_edges.as<int>();
+    a.q_rows = ctx->q_rows.as<int>();
+    a.row_cap = cap;
+    a.logits = ctx->mlp.logits.as<float>();
+    BCC_CUDA(ctx, cudaMemsetAsync(a.q_count, 0, sizeof(int) * ((size_t)grid + 1), st));
+    cudaEvent_t* ev = a.stage_events;
+    if (ev) cudaEventRecord(ev[1], st);
+    BCC_CUDA(ctx, bcc::launch_prep(BCC_ROBOT_PANDA, a, st));
+    if (ev) {
+        cudaEventRecord(ev[2], st);
+        cudaEventRecord(ev[3], st);
+        cudaEventRecord(ev[4], st);
+    }
+    a.mode = 1;
+    BCC_CUDA(ctx, bcc::launch_check_mode(BCC_ROBOT_PANDA, a, st));
+    int rows = 0;
+    BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.row_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    rows = std::min(*ctx->h_total, cap);
+    ctx->last_learned_rows = rows;
+    if (rows > 0) {
+        BCC_CUDA(ctx, bcc::launch_queue_features(BCC_ROBOT_PANDA, a, ctx->env_code.as<float>(),
+                                                 ctx->mlp.x.as<uint16_t>(), grid, st));
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        BCC_CUDA(ctx, bcc::mlp_forward(ctx->mlp.x.as<uint16_t>(), rows, ctx->mlp.images.as<uint8_t>(),
+                                       ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
+                                       std::max(sms, 1), st));
+    }
+    a.mode = 2;
+    BCC_CUDA(ctx, bcc::launch_check_mode(BCC_ROBOT_PANDA, a, st));
+    if (ev) cudaEventRecord(ev[5], st);
+    return BCC_OK;
+}
+
+bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution,
+                     uint8_t* d_results, const bcc_opts* opts, cudaStream_t st) {
+    bcc::PipelineArgs a;
+    bcc_status s = prepare(ctx, robot, d_edges, E, resolution, d_results, opts, st, a);
+    if (s != BCC_OK) return s;
+    if (opts && opts->order == BCC_ORDER_LEARNED) return run_learned(ctx, a, st);
+    BCC_CUDA(ctx, bcc::launch_check((int)robot, a, st));
     return BCC_OK;
 }
 
@@ -450,6 +526,7 @@ bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
     ctx->num_envs = N;
     ctx->max_prims = max_prims;
     ctx->blob_smem = blob_smem;
+    ctx->env_code_ready = false;
     return BCC_OK;
 }
 
@@ -491,5 +568,113 @@ bcc_status bcc_check(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t 
     if (flag) return fail(ctx, BCC_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
     return BCC_OK;
 }
+
+// Train the collision-likelihood MLP on checker-labelled samples drawn from
+// the uploaded environments and the given (host) edges.
+bcc_status bcc_mlp_train(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                         int64_t num_samples, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                         float* h_epoch_loss, float* h_positive_fraction) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs <= 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (!edges || num_edges <= 0 || num_samples <= 0 || epochs <= 0 || batch < 128 || resolution <= 0)
+        return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad training arguments");
+    if (!ctx->mlp.ready) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "set initial MLP parameters first");
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int dof = bcc_robot_dof(robot);
+    if (dof < 0) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "unknown robot");
+    cudaStream_t st = ctx->stream;
+    BCC_CUDA(ctx, ctx->edges.ensure(sizeof(float) * 2 * (size_t)dof * num_edges));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->edges.p, edges, sizeof(float) * 2 * (size_t)dof * num_edges, cudaMemcpyHostToDevice));
+    bcc::PipelineArgs a;
+    bcc_status s = prepare(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, nullptr, nullptr, st, a);
+    if (s != BCC_OK) return s;
+    BCC_CUDA(ctx, bcc::launch_prep((int)robot, a, st));
+    s = ensure_env_code(ctx, st);
+    if (s != BCC_OK) return s;
+    bcc::MlpState& m = ctx->mlp;
+    BCC_CUDA(ctx, m.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)num_samples));
+    BCC_CUDA(ctx, m.y.ensure((size_t)num_samples));
+    BCC_CUDA(ctx, bcc::launch_training_rows((int)robot, a, ctx->env_code.as<float>(), num_samples, seed,
+                                            m.x.as<uint16_t>(), m.y.as<uint8_t>(), st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    if (h_positive_fraction) {
+        std::vector<uint8_t> yy((size_t)num_samples);
+        BCC_CUDA(ctx, cudaMemcpy(yy.data(), m.y.p, yy.size(), cudaMemcpyDeviceToHost));
+        size_t pos = 0;
+        for (uint8_t v : yy) pos += v;
+        *h_positive_fraction = (float)pos / (float)yy.size();
+    }
+    const long long nb = num_samples / batch;
+    for (int ep = 0; ep < epochs; ++ep) {
+        double tot = 0.0;
+        for (long long b = 0; b < nb; ++b) {
+            float loss = 0.0f;
+            s = bcc_mlp_train_step(ctx, m.x.as<uint16_t>() + (size_t)b * batch * bcc::kMlpIn, m.y.as<uint8_t>() + (size_t)b * batch,
+                                   batch, lr, &loss);
+            if (s != BCC_OK) return s;
+            tot += loss;
+        }
+        if (h_epoch_loss) h_epoch_loss[ep] = (float)(tot / (double)(nb * batch));
+    }
+    return BCC_OK;
+}
+
+// Held-out evaluation on fresh samples: metrics[0] mean BCE, [1] misprediction
+// rate (sign of the logit vs the checker's label), [2] false-positive rate,
+// [3] false-negative rate, [4] positive fraction.
+bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                            int64_t num_samples, uint64_t seed, float* h_metrics) {
+    if (!ctx || !h_metrics) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs <= 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (!ctx->mlp.ready || !edges || num_edges <= 0 || num_samples <= 0) return BCC_ERR_INVALID_ARGUMENT;
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int dof = bcc_robot_dof(robot);
+    cudaStream_t st = ctx->stream;
+    BCC_CUDA(ctx, ctx->edges.ensure(sizeof(float) * 2 * (size_t)dof * num_edges));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->edges.p, edges, sizeof(float) * 2 * (size_t)dof * num_edges, cudaMemcpyHostToDevice));
+    bcc::PipelineArgs a;
+    bcc_status s = prepare(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, nullptr, nullptr, st, a);
+    if (s != BCC_OK) return s;
+    BCC_CUDA(ctx, bcc::launch_prep((int)robot, a, st));
+    s = ensure_env_code(ctx, st);
+    if (s != BCC_OK) return s;
+    bcc::MlpState& m = ctx->mlp;
+    BCC_CUDA(ctx, m.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)num_samples));
+    BCC_CUDA(ctx, m.y.ensure((size_t)num_samples));
+    BCC_CUDA(ctx, m.logits.ensure(sizeof(float) * (size_t)num_samples));
+    BCC_CUDA(ctx, bcc::launch_training_rows((int)robot, a, ctx->env_code.as<float>(), num_samples, seed,
+                                            m.x.as<uint16_t>(), m.y.as<uint8_t>(), st));
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    BCC_CUDA(ctx, cudaMemsetAsync(a.error_flag, 0, sizeof(int), st));
+    BCC_CUDA(ctx, bcc::mlp_forward(m.x.as<uint16_t>(), (int)num_samples, m.images.as<uint8_t>(), m.params.as<float>(),
+                                   m.logits.as<float>(), a.error_flag, std::max(sms, 1), st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    std::vector<uint8_t> yy((size_t)num_samples);
+    std::vector<float> zz((size_t)num_samples);
+    BCC_CUDA(ctx, cudaMemcpy(yy.data(), m.y.p, yy.size(), cudaMemcpyDeviceToHost));
+    BCC_CUDA(ctx, cudaMemcpy(zz.data(), m.logits.p, zz.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    double loss = 0;
+    long long wrong = 0, fp = 0, fn = 0, pos = 0;
+    for (size_t i = 0; i < yy.size(); ++i) {
+        const double z = zz[i], y = yy[i];
+        loss += std::max(z, 0.0) - z * y + std::log1p(std::exp(-std::fabs(z)));
+        const bool pred = z > 0;
+        pos += yy[i];
+        if (pred != (yy[i] != 0)) {
+            ++wrong;
+            if (pred) ++fp; else ++fn;
+        }
+    }
+    const double n = (double)yy.size();
+    h_metrics[0] = (float)(loss / n);
+    h_metrics[1] = (float)(wrong / n);
+    h_metrics[2] = (float)(fp / n);
+    h_metrics[3] = (float)(fn / n);
+    h_metrics[4] = (float)(pos / n);
+    return BCC_OK;
+}
+
+int64_t bcc_last_learned_rows(const bcc_ctx* ctx) { return ctx ? ctx->last_learned_rows : -1; }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -63,4 +64,7 @@ struct bcc_ctx {
     // learned proposal
     bcc::MlpState mlp;
     bcc::DevBuf env_code;    // [num_envs][32] environment encodings
+    bool env_code_ready = false;
+    bcc::DevBuf q_count, q_edges, q_rows;  // learned-order queue of undecided pairs
+    long long last_learned_rows = 0;       // MLP rows scored by the last learned check
 };

@@ -23,6 +23,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <cuda_bf16.h>
+
 #include "bcc_device.cuh"
 #include "bcc_kernels.h"
 #include "robot_panda.h"
@@ -39,6 +41,7 @@ struct DevTables {
     int self_pair_begin[M::num_self_groups + 1];
     unsigned char self_pairs[M::num_self_pairs][2];
     float sphere_radius[M::num_spheres];
+    float s_m[M::dof], s_a[M::dof];  // joint-limit scale q = u * s_m + s_a
 };
 
 __constant__ DevTables<PandaModel> c_tab_panda;
@@ -67,6 +70,10 @@ static DevTables<M> host_tables() {
         t.self_pairs[i][1] = (unsigned char)M::table_pos[M::self_pairs[i][1]];
     }
     for (int s = 0; s < M::num_spheres; ++s) t.sphere_radius[s] = M::sphere_radius[s];
+    for (int j = 0; j < M::dof; ++j) {
+        t.s_m[j] = M::s_m[j];
+        t.s_a[j] = M::s_a[j];
+    }
     return t;
 }
 
@@ -258,16 +265,24 @@ __device__ __forceinline__ int slab_tri(float lo, float hi, float g0, float inv)
     return tri_index(i0, i1);
 }
 
-template <class M, int WARPS>
+// MODE 0: plain order, full walk.  MODE 1 (learned pipeline, phase 1): plain
+// order, first 32-item chunk only; a pair still undecided after it is queued
+// (with MLP rows for its segments) instead of getting a verdict.  MODE 2
+// (phase 3): the CTA's queued pairs, walked in descending segment score.
+template <class M, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
     constexpr int G = M::num_env_groups;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
+    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
 
     const int env = blockIdx.x;
     const int e_begin = blockIdx.y * P.edges_per_cta;
     const int e_end = min(e_begin + P.edges_per_cta, P.num_edges);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cta = blockIdx.y * gridDim.x + blockIdx.x;
+    const int n_slots = MODE == 2 ? P.q_count[cta] : e_end - e_begin;
+    if (n_slots <= 0) return;
 
     // Environment header: grid origin, inverse slab width, blob offset and shape.
     const float4 h0 = P.env_hdr[2 * env + 0];
@@ -299,7 +314,8 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
     }
     const DevTables<M>& T = tab<M>();
 
-    for (int e = e_begin + warp; e < e_end; e += WARPS) {
+    for (int slot = warp; slot < n_slots; slot += WARPS) {
+        const int e = MODE == 2 ? P.q_edges[(size_t)cta * P.edges_per_cta + slot] : e_begin + slot;
         uint8_t* out = P.results + (size_t)e * P.num_envs + env;
         const int self = P.edge_self[e];
         if (np == 0 || self) {  // a self-colliding sample collides in every environment
@@ -341,19 +357,40 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
         __syncwarp();
 
         // Walk (sample rank, pair) items, 32 per step, in check order.
-        bool collide = false;
+        bool collide = false, undecided = false;
         unsigned long long n_chunks = 0, n_gates = 0, n_leaf = 0;
         if (C > 0) {
             const int n = P.steps[e];
             const int total = kLanes * n * C;
             const size_t row0 = (size_t)P.offs[e];
+            // Learned order: rank the edge's 4 n segments by their MLP score
+            // (descending, ties by index; NaN scores last).
+            const int nseg = 4 * n;
+            const int seg_row = MODE == 2 ? P.q_rows[(size_t)cta * P.edges_per_cta + slot] : -1;
+            const bool learned = MODE == 2 && seg_row >= 0 && nseg <= kMaxSegments;
+            if (learned) {
+                float v0 = lane < nseg ? P.logits[seg_row + lane] : -INFINITY;
+                float v1 = lane + 32 < nseg ? P.logits[seg_row + lane + 32] : -INFINITY;
+                v0 = isnan(v0) ? -INFINITY : v0;
+                v1 = isnan(v1) ? -INFINITY : v1;
+                int rank0 = 0, rank1 = 0;
+                for (int i = 0; i < nseg; ++i) {
+                    const float vi = __shfl_sync(0xffffffffu, i < 32 ? v0 : v1, i & 31);
+                    rank0 += (vi > v0 || (vi == v0 && i < lane)) ? 1 : 0;
+                    rank1 += (vi > v1 || (vi == v1 && i < lane + 32)) ? 1 : 0;
+                }
+                if (lane < nseg) s_perm[warp][rank0] = (uint8_t)lane;
+                if (lane + 32 < nseg) s_perm[warp][rank1] = (uint8_t)(lane + 32);
+                __syncwarp();
+            }
             const int dr = 32 / C, dc = 32 % C;
             int r = lane / C, c = lane - (lane / C) * C;
             for (int w0 = 0; w0 < total; w0 += 32) {
                 bool gate = false;
                 int g = 0, p = 0, k = 0;
                 if (w0 + lane < total) {
-                    k = reference_rank_to_sample(r, n);
+                    k = learned ? (int)s_perm[warp][r >> 3] * kSegment + (r & (kSegment - 1))
+                                : reference_rank_to_sample(r, n);
                     const uint32_t pr = pairs[c];
                     g = (int)(pr & 15u);
                     p = (int)(pr >> 4);
@@ -405,6 +442,10 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
                     }
                     if (collide) break;
                 }
+                if (MODE == 1 && w0 + 32 < total) {  // probe: one chunk only
+                    undecided = true;
+                    break;
+                }
                 c += dc;
                 r += dr;
                 if (c >= C) {
@@ -414,6 +455,20 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
             }
         }
         __syncwarp();
+        if (MODE == 1 && undecided) {
+            if (lane == 0) {
+                const int n = P.steps[e];
+                const int qi = atomicAdd(P.q_count + cta, 1);
+                int ro = -1;
+                if (4 * n <= kMaxSegments) {
+                    ro = atomicAdd(P.row_count, 4 * n);
+                    if (ro > P.row_cap - 4 * n) ro = -1;
+                }
+                P.q_edges[(size_t)cta * P.edges_per_cta + qi] = e;
+                P.q_rows[(size_t)cta * P.edges_per_cta + qi] = ro;
+            }
+            continue;
+        }
         if (lane == 0) {
             *out = collide ? 1 : 0;
             if (P.counters) {
@@ -443,16 +498,25 @@ static cudaError_t run_steps(const PipelineArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <class M, int W>
-static cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st) {
+template <class M, int W, int MODE>
+static cudaError_t launch_check_wm(CheckParams P, int E, cudaStream_t st) {
     P.pairs_per_warp = (P.max_prims * M::num_env_groups + 7) & ~7;
     const size_t smem = P.blob_smem + (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
-    cudaError_t err = cudaFuncSetAttribute(check_kernel<M, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t err = cudaFuncSetAttribute(check_kernel<M, W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
     if (err != cudaSuccess) return err;
     dim3 grid(P.num_envs, (E + P.edges_per_cta - 1) / P.edges_per_cta);
-    check_kernel<M, W><<<grid, W * 32, smem, st>>>(P);
+    check_kernel<M, W, MODE><<<grid, W * 32, smem, st>>>(P);
     return cudaGetLastError();
+}
+
+template <class M, int W>
+static cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st, int mode) {
+    switch (mode) {
+        case 1: return launch_check_wm<M, W, 1>(P, E, st);
+        case 2: return launch_check_wm<M, W, 2>(P, E, st);
+        default: return launch_check_wm<M, W, 0>(P, E, st);
+    }
 }
 
 template <class M>
@@ -488,11 +552,17 @@ static cudaError_t run_check(const PipelineArgs& a, cudaStream_t st) {
     P.results = a.d_results;
     P.error_flag = a.error_flag;
     P.counters = a.counters;
+    P.q_count = a.q_count;
+    P.q_edges = a.q_edges;
+    P.q_rows = a.q_rows;
+    P.row_count = a.row_count;
+    P.row_cap = a.row_cap;
+    P.logits = a.logits;
     switch (a.warps) {
-        case 8: err = launch_check_w<M, 8>(P, E, st); break;
-        case 4: err = launch_check_w<M, 4>(P, E, st); break;
-        case 2: err = launch_check_w<M, 2>(P, E, st); break;
-        case 1: err = launch_check_w<M, 1>(P, E, st); break;
+        case 8: err = launch_check_w<M, 8>(P, E, st, a.mode); break;
+        case 4: err = launch_check_w<M, 4>(P, E, st, a.mode); break;
+        case 2: err = launch_check_w<M, 2>(P, E, st, a.mode); break;
+        case 1: err = launch_check_w<M, 1>(P, E, st, a.mode); break;
         default: return cudaErrorInvalidValue;
     }
     if (ev) cudaEventRecord(ev[5], st);
@@ -512,6 +582,246 @@ cudaError_t launch_check(int robot, const PipelineArgs& a, cudaStream_t st) {
 int robot_num_spheres(int robot) { return robot == 0 ? PandaModel::num_spheres : -1; }
 int robot_num_env_groups(int robot) { return robot == 0 ? PandaModel::num_env_groups : -1; }
 int robot_dof(int robot) { return robot == 0 ? PandaModel::dof : -1; }
+
+}  // namespace bcc
+
+// ======================================================================
+// Learned check order: environment code, MLP features, training rows.
+// ======================================================================
+namespace bcc {
+
+// 32-value environment code (one warp per environment): [0..3] counts of
+// sphere-like, capsule-like and box-like primitives and the total, / 64;
+// [4..27] for 8 fixed anchor points the distance from the anchor to the
+// nearest primitive of each of the three kinds (clamped to [-0.5, 1.5] m);
+// [28..31] mean primitive centre xyz and mean extent.
+__device__ __forceinline__ float prim_point_dist(const float4* rec, float x, float y, float z) {
+    const float4 w0 = rec[0], w1 = rec[1], w2 = rec[2], w3 = rec[3];
+    const float dx = x - w0.x, dy = y - w0.y, dz = z - w0.z;
+    const float e1 = fmaxf(fabsf(w1.x * dx + w1.y * dy + w1.z * dz) - w1.w, 0.0f);
+    const float e2 = fmaxf(fabsf(w2.x * dx + w2.y * dy + w2.z * dz) - w2.w, 0.0f);
+    const float e3 = fmaxf(fabsf(w3.x * dx + w3.y * dy + w3.z * dz) - w3.w, 0.0f);
+    return sqrtf(e1 * e1 + e2 * e2 + e3 * e3) - w0.w;
+}
+
+__global__ void env_encode_kernel(const float4* __restrict__ blobs, const float4* __restrict__ hdr, int N,
+                                  float* __restrict__ code) {
+    const int env = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (env >= N) return;
+    const float4 h0 = hdr[2 * env], h1 = hdr[2 * env + 1];
+    const float4* rec = blobs + __float_as_uint(h0.w);
+    const int np = (int)(__float_as_uint(h1.w) & 0xffffu);
+    float cnt[3] = {0, 0, 0}, best[8][3], mean[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < 8; ++a) best[a][0] = best[a][1] = best[a][2] = 1.5f;
+    for (int p = lane; p < np; p += 32) {
+        const float4* r = rec + p * kPrimF4;
+        const float4 w0 = r[0];
+        const float hsum = r[1].w + r[2].w + r[3].w;
+        const int kind = w0.w > 0.0f ? (hsum > 0.0f ? 1 : 0) : 2;  // sphere, capsule, box
+        cnt[kind] += 1.0f;
+        mean[0] += w0.x;
+        mean[1] += w0.y;
+        mean[2] += w0.z;
+        mean[3] += w0.w + hsum;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const float ax = (a & 1) ? 0.35f : -0.35f, ay = (a & 2) ? 0.35f : -0.35f, az = (a & 4) ? 0.8f : 0.3f;
+            best[a][kind] = fminf(best[a][kind], prim_point_dist(r, ax, ay, az));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) cnt[k] += __shfl_xor_sync(0xffffffffu, cnt[k], o);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) mean[k] += __shfl_xor_sync(0xffffffffu, mean[k], o);
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) best[a][k] = fminf(best[a][k], __shfl_xor_sync(0xffffffffu, best[a][k], o));
+    }
+    if (lane == 0) {
+        float* c = code + (size_t)env * 32;
+        c[0] = cnt[0] / 64.0f;
+        c[1] = cnt[1] / 64.0f;
+        c[2] = cnt[2] / 64.0f;
+        c[3] = (float)np / 64.0f;
+        for (int a = 0; a < 8; ++a)
+            for (int k = 0; k < 3; ++k) c[4 + a * 3 + k] = fminf(fmaxf(best[a][k], -0.5f), 1.5f);
+        const float inv = np > 0 ? 1.0f / (float)np : 0.0f;
+        for (int k = 0; k < 4; ++k) c[28 + k] = mean[k] * inv;
+    }
+}
+
+// One MLP feature row: joints normalised to [-1, 1] by the joint limits, the
+// environment code, zeros; BF16, 48 values (96 bytes).
+template <class M>
+__device__ __forceinline__ void write_features(const float* q, const float* code, uint16_t* dst) {
+    const DevTables<M>& T = tab<M>();
+    float f[48];
+#pragma unroll
+    for (int j = 0; j < 48; ++j) f[j] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < M::dof; ++j) f[j] = 2.0f * (q[j] - T.s_a[j]) / T.s_m[j] - 1.0f;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) f[7 + j] = code[j];
+    uint32_t w[24];
+#pragma unroll
+    for (int j = 0; j < 24; ++j) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+        w[j] = *reinterpret_cast<uint32_t*>(&h);
+    }
+    uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) d[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+}
+
+// Features of every queued pair's segments: row ro + j is segment j scored at
+// its middle sample k = 8 j + 4.  One warp per queued pair.
+template <class M>
+__global__ void queue_features_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
+                                      uint16_t* __restrict__ x) {
+    const int cta = blockIdx.x;
+    const int env = cta % P.num_envs;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nq = P.q_count[cta];
+    for (int slot = warp; slot < nq; slot += blockDim.x >> 5) {
+        const int ro = P.q_rows[(size_t)cta * P.edges_per_cta + slot];
+        if (ro < 0) continue;
+        const int e = P.q_edges[(size_t)cta * P.edges_per_cta + slot];
+        const int n = P.steps[e];
+        float s[M::dof], t[M::dof], q[M::dof];
+#pragma unroll
+        for (int j = 0; j < M::dof; ++j) {
+            s[j] = edges[(size_t)e * 2 * M::dof + j];
+            t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
+        }
+        for (int seg = lane; seg < 4 * n; seg += 32) {
+            edge_sample<M::dof>(s, t, n, seg * kSegment + kSegment / 2, q);
+            write_features<M>(q, code + (size_t)env * 32, x + (size_t)(ro + seg) * 48);
+        }
+    }
+}
+
+// Training rows: row i draws (environment, edge, sample) from a hash of
+// (seed, i); features as above at that sample; label = the sample's
+// environment collision (gate then leaves, every primitive).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+template <class M>
+__global__ void training_rows_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
+                                     long long rows, unsigned long long seed, uint16_t* __restrict__ x,
+                                     uint8_t* __restrict__ y) {
+    constexpr int G = M::num_env_groups;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const unsigned long long h1 = mix64(seed ^ (unsigned long long)i), h2 = mix64(h1), h3 = mix64(h2);
+    const int env = (int)(h1 % (unsigned long long)P.num_envs);
+    const int e = (int)(h2 % (unsigned long long)P.num_edges);
+    const int n = P.steps[e];
+    const int k = (int)(h3 % (unsigned long long)(kLanes * n));
+    float s[M::dof], t[M::dof], q[M::dof];
+#pragma unroll
+    for (int j = 0; j < M::dof; ++j) {
+        s[j] = edges[(size_t)e * 2 * M::dof + j];
+        t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
+    }
+    edge_sample<M::dof>(s, t, n, k, q);
+    write_features<M>(q, code + (size_t)env * 32, x + (size_t)i * 48);
+    const float4 hd0 = P.env_hdr[2 * env], hd1 = P.env_hdr[2 * env + 1];
+    const float4* rec = P.blobs + __float_as_uint(hd0.w);
+    const int np = (int)(__float_as_uint(hd1.w) & 0xffffu);
+    const float4* row = P.table + ((size_t)P.offs[e] + k) * M::num_spheres;
+    const DevTables<M>& T = tab<M>();
+    bool hit = false;
+    for (int p = 0; p < np && !hit; ++p) {
+        const float4* r = rec + p * kPrimF4;
+        for (int g = 0; g < G && !hit; ++g) {
+            float4 b = row[g];
+            b.w += kEnvInflate;
+            if (!sphere_hits_prim(b, r)) continue;
+            for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1] && !hit; ++li) {
+                float4 l = row[G + li];
+                l.w += kEnvInflate;
+                hit = sphere_hits_prim(l, r);
+            }
+        }
+    }
+    y[i] = hit ? 1 : 0;
+}
+
+int check_grid_size(const PipelineArgs& a) {
+    return a.num_envs * ((a.num_edges + a.edges_per_cta - 1) / a.edges_per_cta);
+}
+
+static CheckParams params_of(const PipelineArgs& a) {
+    CheckParams P{};
+    P.blobs = a.blobs;
+    P.env_hdr = a.env_hdr;
+    P.num_envs = a.num_envs;
+    P.num_edges = a.num_edges;
+    P.max_prims = a.max_prims;
+    P.blob_smem = a.blob_smem;
+    P.edges_per_cta = a.edges_per_cta;
+    P.steps = a.steps;
+    P.offs = a.offs;
+    P.table = a.table;
+    P.swept = a.swept;
+    P.edge_self = a.edge_self;
+    P.results = a.d_results;
+    P.error_flag = a.error_flag;
+    P.q_count = a.q_count;
+    P.q_edges = a.q_edges;
+    P.q_rows = a.q_rows;
+    P.row_count = a.row_count;
+    P.row_cap = a.row_cap;
+    P.logits = a.logits;
+    return P;
+}
+
+// Environment check only (the FK/self/swept stages already ran), in a.mode.
+cudaError_t launch_check_mode(int robot, const PipelineArgs& a, cudaStream_t st) {
+    if (robot != 0) return cudaErrorInvalidValue;
+    using M = PandaModel;
+    CheckParams P = params_of(a);
+    switch (a.warps) {
+        case 8: return launch_check_w<M, 8>(P, a.num_edges, st, a.mode);
+        case 4: return launch_check_w<M, 4>(P, a.num_edges, st, a.mode);
+        case 2: return launch_check_w<M, 2>(P, a.num_edges, st, a.mode);
+        case 1: return launch_check_w<M, 1>(P, a.num_edges, st, a.mode);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st) {
+    if (num_envs <= 0) return cudaSuccess;
+    env_encode_kernel<<<(num_envs * 32 + 255) / 256, 256, 0, st>>>(blobs, env_hdr, num_envs, code);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_queue_features(int robot, const PipelineArgs& a, const float* env_code, uint16_t* x, int grid,
+                                  cudaStream_t st) {
+    if (robot != 0) return cudaErrorInvalidValue;
+    if (grid <= 0) return cudaSuccess;
+    queue_features_kernel<PandaModel><<<grid, 128, 0, st>>>(params_of(a), a.d_edges, env_code, x);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_training_rows(int robot, const PipelineArgs& a, const float* env_code, long long rows,
+                                 unsigned long long seed, uint16_t* x, uint8_t* y, cudaStream_t st) {
+    if (robot != 0) return cudaErrorInvalidValue;
+    if (rows <= 0) return cudaSuccess;
+    training_rows_kernel<PandaModel><<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(params_of(a), a.d_edges, env_code,
+                                                                                  rows, seed, x, y);
+    return cudaGetLastError();
+}
 
 }  // namespace bcc
 

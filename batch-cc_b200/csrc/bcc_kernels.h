@@ -35,7 +35,19 @@ struct CheckParams {
     uint8_t* results;        // [E][num_envs]
     int* error_flag;         // set when a bounded wait gives up
     unsigned long long* counters;  // null, or kNumCounters work counters (diagnostics)
+    // Learned order (modes 1 and 2 of the check kernel); unused in plain mode.
+    int* q_count;            // [grid] queued edges of each CTA
+    int* q_edges;            // [grid][edges_per_cta] queued edge ids
+    int* q_rows;             // [grid][edges_per_cta] first MLP row of the entry, -1 = none
+    int* row_count;          // rows handed out so far
+    int row_cap;             // capacity of the MLP row buffers
+    const float* logits;     // [row_cap] segment scores (mode 2)
 };
+
+// Samples per learned-order segment: the MLP scores each run of 8 consecutive
+// samples at its middle sample; an edge with step count n has 4 n segments.
+constexpr int kSegment = 8;
+constexpr int kMaxSegments = 64;  // edges with more segments keep the plain order
 
 // Work counters of the environment check (diagnostics, off by default):
 // pairs walked, candidate (primitive, link) pairs, 32-item chunks, gate steps
@@ -64,7 +76,24 @@ struct PipelineArgs {
     int* error_flag;
     cudaEvent_t* stage_events;  // null, or 6 events bracketing the 5 stages
     unsigned long long* counters;
+    int mode;                // 0 plain, 1 probe (first chunk, queue the rest), 2 finish (learned order)
+    int* q_count;
+    int* q_edges;
+    int* q_rows;
+    int* row_count;
+    int row_cap;
+    const float* logits;
 };
+
+cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st);
+// Learned-order helpers (bcc_kernels.cu).
+cudaError_t launch_check_mode(int robot, const PipelineArgs& a, cudaStream_t st);
+cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st);
+cudaError_t launch_queue_features(int robot, const PipelineArgs& a, const float* env_code, uint16_t* x, int grid,
+                                  cudaStream_t st);
+cudaError_t launch_training_rows(int robot, const PipelineArgs& a, const float* env_code, long long rows,
+                                 unsigned long long seed, uint16_t* x, uint8_t* y, cudaStream_t st);
+int check_grid_size(const PipelineArgs& a);
 
 // Environment check from host-packed records (bcc_pack_envs format), exact
 // AABB cull; used by the allocation-free entry point.

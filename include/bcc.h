@@ -196,6 +196,23 @@ bcc_status bcc_mlp_forward(bcc_ctx* ctx, const void* d_x_bf16, int32_t rows, flo
  * summed loss (may be NULL). */
 bcc_status bcc_mlp_gradients(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows,
                              float* h_grads, float* h_loss);
+/*
+ * Train on checker-labelled samples: num_samples (environment, edge, sample)
+ * triples drawn (seeded) from the uploaded environments and the given host
+ * edges; label = the sample's environment collision by this library's check.
+ * Adam, `epochs` passes in batches of `batch` rows.  h_epoch_loss[epochs]: mean
+ * loss per epoch (may be NULL); h_positive_fraction: label balance (may be NULL).
+ */
+bcc_status bcc_mlp_train(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                         int64_t num_samples, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                         float* h_epoch_loss, float* h_positive_fraction);
+/* Held-out metrics on fresh samples: [0] mean BCE, [1] misprediction rate (sign
+ * of the logit vs the checker's verdict), [2] false-positive rate, [3]
+ * false-negative rate, [4] positive fraction. */
+bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                            int64_t num_samples, uint64_t seed, float* h_metrics);
+/* MLP rows (segments) scored by the last learned-order check. */
+int64_t bcc_last_learned_rows(const bcc_ctx* ctx);
 /* One Adam step (learning rate lr) on the gradient of the batch. */
 bcc_status bcc_mlp_train_step(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows,
                               float lr, float* h_loss);

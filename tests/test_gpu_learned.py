@@ -1,0 +1,61 @@
+"""GPU tests of the learned check order: the trained proposal never changes a
+verdict, it is trained by the project's tensor-core kernels on checker labels,
+its misprediction rate is measured, and it reduces the work spent on the pairs
+a plain first chunk leaves undecided."""
+import numpy as np
+import pytest
+
+from bcc import mlp, workload
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def trained(checker):
+    train_envs = workload.gen_envs("stress", 64, seed=101)
+    train_edges = workload.gen_edges("stress", 3000, seed=101)
+    checker.mlp_set_params(mlp.init_params(7))
+    checker.upload(train_envs)
+    losses, pos = checker.mlp_train(train_edges, num_samples=1 << 19, epochs=3, batch=8192, lr=2e-3, seed=11)
+    metrics = checker.mlp_evaluate(workload.gen_edges("stress", 1000, seed=102), 1 << 16, seed=12)
+    return dict(losses=losses, pos=pos, metrics=metrics, params=checker.mlp_get_params())
+
+
+def test_training_learns(trained):
+    losses, m = trained["losses"], trained["metrics"]
+    assert losses[-1] < losses[0]
+    base = min(m["positive"], 1 - m["positive"])  # error of the constant predictor
+    assert m["mispredict"] < base, (m, base)
+
+
+@pytest.mark.parametrize("name,nenv,nedge,seed", [("stress", 30, 400, 21), ("uneven", 30, 300, 22)])
+def test_learned_order_keeps_verdicts(checker, trained, name, nenv, nedge, seed):
+    checker.mlp_set_params(trained["params"])
+    envs = workload.gen_envs(name, nenv, seed=seed)
+    edges = workload.gen_edges(name, nedge, seed=seed)
+    checker.upload(envs)
+    plain = checker.check(edges, order="plain")
+    learned = checker.check(edges, order="learned")
+    assert checker.last_learned_rows() > 0
+    # Same tests in a different order: identical verdicts.
+    assert np.array_equal(plain, learned)
+    n_mis, n_adj, bad = orc.adjudicate(envs, edges, learned, orc.check(envs, edges))
+    assert len(bad) == 0
+
+
+def test_trained_network_saves_work(checker, trained):
+    """Chunks walked on the stress workload: trained proposal vs the same
+    pipeline with an untrained network (the method without the learning)."""
+    envs = workload.gen_envs("stress", 40, seed=31)
+    edges = workload.gen_edges("stress", 1500, seed=31)
+    checker.upload(envs)
+    checker.set_profiling(True, counters=True)
+    work = {}
+    for label, params in (("untrained", mlp.init_params(99)), ("trained", trained["params"])):
+        checker.mlp_set_params(params)
+        checker.check(edges, order="learned")
+        work[label] = checker.work_counters()
+    checker.set_profiling(False)
+    assert work["trained"]["colliding"] == work["untrained"]["colliding"]
+    assert work["trained"]["chunks"] <= work["untrained"]["chunks"], work
