@@ -40,7 +40,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--ref-path", default="cpu", choices=["cpu", "cuda"])
-    p.add_argument("--order", default="plain", choices=["plain", "learned"])
+    p.add_argument("--order", default="learned", choices=["plain", "learned"],
+                   help="order whose throughput is the headline value (both are timed)")
+    p.add_argument("--train-samples", type=int, default=10_000_000)
+    p.add_argument("--train-epochs", type=int, default=2)
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--flop-sample", type=int, default=20000)
@@ -206,6 +209,67 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def train_proposal(chk, args):
+    """Train the collision-likelihood MLP (untimed) on checker labels of
+    uneven-style environments and edges with seeds disjoint from the benchmark's."""
+    from bcc import mlp, workload
+    t0 = time.perf_counter()
+    chk.upload(workload.gen_envs(args.workload, args.envs, seed=1000))
+    chk.mlp_set_params(mlp.init_params(1000))
+    losses, pos = chk.mlp_train(workload.gen_edges(args.workload, args.edges, seed=1000),
+                                num_samples=args.train_samples, epochs=args.train_epochs, batch=16384, lr=2e-3,
+                                seed=1000)
+    return {"train_samples": args.train_samples, "epochs": args.train_epochs, "epoch_loss": [float(v) for v in losses],
+            "train_positive_fraction": pos, "train_seconds": time.perf_counter() - t0,
+            "data": "checker-labelled samples of %s environments/edges with seed 1000 (benchmark uses seed 0)" % (
+                args.workload)}
+
+
+def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev):
+    import torch
+
+    def step():
+        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    stage_tot, check_ms = {}, []
+    for i in range(steps):
+        flush.fill_(float(i))  # evict L2 between timed iterations (untimed)
+        evs[i][0].record(stream)
+        step()
+        evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        st = chk.stage_times()
+        check_ms.append(st["check"])
+        for k, v in st.items():
+            stage_tot[k] = stage_tot.get(k, 0.0) + v
+    total_ms = sum(x.elapsed_time(y) for x, y in evs)
+    return total_ms, check_ms, {k: v / steps for k, v in stage_tot.items()}
+
+
+def mlp_roofline(chk, dev, rows=1 << 22, reps=5):
+    """tcgen05 MLP forward kernel alone: 2 * rows * (48*128 + 2*128*128 + 128) FLOP per launch."""
+    import torch
+    x = torch.randint(-2000, 2000, (rows, 48), dtype=torch.int16, device=f"cuda:{dev}")
+    x[:, 39:] = 0
+    out = torch.empty(rows, dtype=torch.float32, device=f"cuda:{dev}")
+    s = torch.cuda.current_stream()
+    chk.mlp_forward_device(x.data_ptr(), rows, out.data_ptr(), stream=s.cuda_stream)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(reps):
+        chk.mlp_forward_device(x.data_ptr(), rows, out.data_ptr(), stream=s.cuda_stream)
+    b.record(s)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    flops = 2.0 * rows * (48 * 128 + 2 * 128 * 128 + 128)
+    return ms, flops / (ms * 1e-3) / 1e12
+
+
 def run_ours(args, world, rank, local, dist):
     import torch
     from bcc import workload
@@ -213,95 +277,111 @@ def run_ours(args, world, rank, local, dist):
 
     dev = local
     torch.cuda.set_device(dev)
+    chk = Checker(dev)
+    proposal = train_proposal(chk, args)
     envs = workload.gen_envs(args.workload, args.envs, seed=0)
     edges = workload.gen_edges(args.workload, args.edges, seed=rank)
     N, E = envs.num_envs, len(edges)
-    chk = Checker(dev)
     chk.upload(envs)
+    proposal.update(chk.mlp_evaluate(edges, 1 << 20, seed=7))
     chk.set_profiling(True)
     stream = torch.cuda.current_stream()
-    sptr = stream.cuda_stream
     d_edges = torch.from_numpy(edges).to(f"cuda:{dev}")
     d_res = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
+    d_res2 = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
-    def step():
-        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=args.order, stream=sptr)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    check_ms = []
-    stage_tot = {}
+    results = {}
     with ClockSampler(dev) as clk:
-        for i in range(args.steps):
-            flush.fill_(float(i))  # evict L2 between timed iterations (untimed)
-            evs[i][0].record(stream)
-            step()
-            evs[i][1].record(stream)
-            torch.cuda.synchronize()
-            st = chk.stage_times()
-            check_ms.append(st["check"])
-            for k, v in st.items():
-                stage_tot[k] = stage_tot.get(k, 0.0) + v
+        for order in ("plain", "learned"):
+            results[order] = time_order(chk, d_edges, d_res, E, order, stream, args.steps, args.warmup, flush, dev)
     torch.cuda.synchronize()
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{dev}")
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms = total_ms / args.steps
-    value = world * N * E / (ms * 1e-3)
+        return float(t.item())
+
+    ms = {o: max_over_ranks(results[o][0]) / args.steps for o in results}
+    head = args.order
+    value = world * N * E / (ms[head] * 1e-3)
+
+    # Verdict agreement of the two orders (must be identical), and work counters.
+    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="plain", stream=stream.cuda_stream)
+    chk.check_device(d_edges.data_ptr(), E, d_res2.data_ptr(), order="learned", stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    mismatch = int((d_res != d_res2).sum().item())
+    work = {}
+    chk.set_profiling(True, counters=True)
+    for order in ("plain", "learned"):
+        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        c = chk.work_counters()
+        work[order] = {k: v / max(c["pairs"], 1) for k, v in c.items() if k != "pairs"}
+        work[order]["pairs_walked"] = c["pairs"]
+    chk.set_profiling(True)
+    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    learned_rows = chk.last_learned_rows()
 
     # e2e: the public host API (pinned host edges in, verdicts out), per step.
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
     h_res = torch.empty((E, N), dtype=torch.uint8).pin_memory().numpy()
-    chk.check(h_edges, out=h_res, order=args.order)
+    chk.check(h_edges, out=h_res, order=head)
     t_e2e = []
     for _ in range(max(3, min(args.steps, 5))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        chk.check(h_edges, out=h_res, order=args.order)
+        chk.check(h_edges, out=h_res, order=head)
         t_e2e.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(t_e2e)
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(statistics.median(t_e2e))
+    mlp_ms, mlp_tf = mlp_roofline(chk, dev)
 
     if rank != 0:
         chk.close()
         return
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
             "config": {"workload": "%s: panda, %d envs (U{8..64} primitives) x %d edges (log-uniform 0.05-2.0 rad), "
-                                   "resolution 32, order %s" % (args.workload, N, E, args.order),
-                       "envs": N, "edges_per_gpu": E, "order": args.order,
+                                   "resolution 32, %s-ordered" % (args.workload, N, E, head),
+                       "envs": N, "edges_per_gpu": E, "order": head,
                        "l2": "256 MB buffer written between timed steps (untimed)", "parallelism": "dp%d" % world},
-            "stages_ms_per_step": {k: v / args.steps for k, v in stage_tot.items()},
-            "gpu_launches": 6 * args.steps,
+            "orders": {o: {"value": world * N * E / (ms[o] * 1e-3), "ms_per_step": ms[o],
+                           "stages_ms_per_step": results[o][2], "work_per_pair": work[o]} for o in results},
+            "learned_over_plain": ms["plain"] / ms["learned"],
+            "verdict_mismatches_learned_vs_plain": mismatch,
+            "proposal": dict(proposal, scored_segments_per_step=learned_rows),
+            "gpu_launches": (6 + 9) * args.steps,  # plain: 6 launches per step; learned: 9
             "clocks": clk.summary()}
     line["e2e"] = {"value": world * N * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(edges.nbytes),
                    "d2h_bytes_per_step": int(N * E)}
-    # Roofline of the dominant kernel (environment check): algorithmic FLOPs of
-    # the reference plain order per launch / mean CUDA-event duration of the launch.
+    # Roofline of the dominant kernel (environment check, plain order):
+    # algorithmic FLOPs of the reference plain order per launch / mean
+    # CUDA-event duration of the launch.
     peak = measure_fp32_peak(dev)
     flops, rel_err = algorithmic_flops(envs, edges, args.flop_sample)
-    chk_ms = statistics.mean(check_ms)
+    chk_ms = statistics.mean(results["plain"][1])
     achieved = flops / (chk_ms * 1e-3) / 1e12
     line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak, "traffic": None,
-                        "kernel": "check_kernel", "kernel_ms": chk_ms,
+                        "kernel": "check_kernel (plain order)", "kernel_ms": chk_ms,
                         "algorithmic_flops_per_launch": flops, "flop_estimate_rel_stderr": rel_err,
                         "peak_source": "FP32 FMA probe kernel measured in this run (bcc_measure_fp32_peak); "
                                        "MEASURED_PEAKS.json has no FP32 figure",
                         "note": "algorithmic FLOPs = the reference's plain-order work (oracle count); "
                                 "work this kernel skips (hoisted FK/self checks, culling) raises frac"}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
+    line["roofline_mlp"] = {"bound": "tensor", "achieved": mlp_tf, "peak": peaks.get("bf16_tflops", 1590.0),
+                            "unit": "TFLOP/s", "frac": mlp_tf / peaks.get("bf16_tflops", 1590.0),
+                            "kernel": "mlp_forward_kernel (tcgen05, 4M rows)", "kernel_ms": mlp_ms,
+                            "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst) of measured"}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(envs, edges)
     chk.close()
