@@ -232,6 +232,7 @@ bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
     a.q_rows = ctx->q_rows.as<int>();
     a.row_cap = cap;
     a.logits = ctx->mlp.logits.as<float>();
+    a.queue_min_items = ctx->queue_min_items;
     BCC_CUDA(ctx, cudaMemsetAsync(a.q_count, 0, sizeof(int) * ((size_t)grid + 1), st));
     cudaEvent_t* ev = a.stage_events;
     if (ev) cudaEventRecord(ev[1], st);

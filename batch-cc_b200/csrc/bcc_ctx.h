@@ -67,4 +67,5 @@ struct bcc_ctx {
     bool env_code_ready = false;
     bcc::DevBuf q_count, q_edges, q_rows;  // learned-order queue of undecided pairs
     long long last_learned_rows = 0;       // MLP rows scored by the last learned check
+    int queue_min_items = 128;             // learned order: remaining items that justify scoring
 };

@@ -442,7 +442,9 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
                     }
                     if (collide) break;
                 }
-                if (MODE == 1 && w0 + 32 < total) {  // probe: one chunk only
+                // Probe: after the first chunk, queue the pair for the learned order
+                // only when much work remains; small remainders finish in plain order.
+                if (MODE == 1 && w0 == 0 && total - 32 >= P.queue_min_items) {
                     undecided = true;
                     break;
                 }
@@ -783,6 +785,8 @@ static CheckParams params_of(const PipelineArgs& a) {
     P.row_count = a.row_count;
     P.row_cap = a.row_cap;
     P.logits = a.logits;
+    P.counters = a.counters;
+    P.queue_min_items = a.queue_min_items;
     return P;
 }
 

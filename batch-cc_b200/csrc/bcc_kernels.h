@@ -42,6 +42,7 @@ struct CheckParams {
     int* row_count;          // rows handed out so far
     int row_cap;             // capacity of the MLP row buffers
     const float* logits;     // [row_cap] segment scores (mode 2)
+    int queue_min_items;     // probe: queue only pairs with at least this many items left
 };
 
 // Samples per learned-order segment: the MLP scores each run of 8 consecutive
@@ -83,6 +84,7 @@ struct PipelineArgs {
     int* row_count;
     int row_cap;
     const float* logits;
+    int queue_min_items;
 };
 
 cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st);

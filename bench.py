@@ -44,6 +44,7 @@ def parse():
                    help="order whose throughput is the headline value (both are timed)")
     p.add_argument("--train-samples", type=int, default=10_000_000)
     p.add_argument("--train-epochs", type=int, default=2)
+    p.add_argument("--train-envs", type=int, default=4000)
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--flop-sample", type=int, default=20000)
@@ -214,7 +215,7 @@ def train_proposal(chk, args):
     uneven-style environments and edges with seeds disjoint from the benchmark's."""
     from bcc import mlp, workload
     t0 = time.perf_counter()
-    chk.upload(workload.gen_envs(args.workload, args.envs, seed=1000))
+    chk.upload(workload.gen_envs(args.workload, args.train_envs, seed=1000))
     chk.mlp_set_params(mlp.init_params(1000))
     losses, pos = chk.mlp_train(workload.gen_edges(args.workload, args.edges, seed=1000),
                                 num_samples=args.train_samples, epochs=args.train_epochs, batch=16384, lr=2e-3,
