@@ -74,6 +74,10 @@ def lib():
                                        ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
         L.bcc_last_learned_rows.argtypes = [vp]
         L.bcc_last_learned_rows.restype = ctypes.c_int64
+        L.bcc_get_launch_config.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+        L.bcc_set_launch_config.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+        L.bcc_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
         L.bcc_set_profiling.argtypes = [vp, ctypes.c_int32]
         L.bcc_work_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32]
         L.bcc_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
@@ -127,13 +131,13 @@ class Checker:
         self._raise(lib().bcc_upload_envs(self._h, ctypes.byref(soa)))
         self.num_envs = envset.num_envs
 
-    def check(self, edges, resolution=32, robot="panda", order="plain", out=None, tile=0):
+    def check(self, edges, resolution=32, robot="panda", order="plain", out=None, tile=0, graph=False):
         """Host API: edges float32 [E, 2, dof] -> verdicts uint8 [E, num_envs]."""
         edges = np.ascontiguousarray(edges, np.float32)
         E = edges.shape[0]
         if out is None:
             out = np.zeros((E, self.num_envs), np.uint8)
-        opts = make_opts(order, tile=tile)
+        opts = make_opts(order, use_graph=graph, tile=tile)
         st = lib().bcc_check(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                              E, resolution, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
                              ctypes.byref(opts))
@@ -212,10 +216,30 @@ class Checker:
     def last_learned_rows(self):
         return int(lib().bcc_last_learned_rows(self._h))
 
+    CONFIG = ("edges_per_cta", "warps", "persistent", "queue_min_items")
+
+    def launch_config(self):
+        c = (ctypes.c_int32 * 4)()
+        self._raise(lib().bcc_get_launch_config(self._h, c))
+        return dict(zip(self.CONFIG, list(c)))
+
+    def set_launch_config(self, **kw):
+        cfg = self.launch_config()
+        cfg.update(kw)
+        c = (ctypes.c_int32 * 4)(*[int(cfg[k]) for k in self.CONFIG])
+        self._raise(lib().bcc_set_launch_config(self._h, c))
+
+    def autotune(self, edges, order="plain", resolution=32, robot="panda"):
+        edges = np.ascontiguousarray(edges, np.float32)
+        c = (ctypes.c_int32 * 4)()
+        self._raise(lib().bcc_autotune(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                       len(edges), resolution, ORDERS[order], c))
+        return dict(zip(self.CONFIG, list(c)))
+
     def check_device(self, d_edges_ptr, num_edges, d_results_ptr, resolution=32, robot="panda",
-                     order="plain", stream=0, tile=0):
+                     order="plain", stream=0, tile=0, graph=False):
         """Device API: raw device pointers (e.g. torch tensors' data_ptr()), stream-ordered."""
-        opts = make_opts(order, tile=tile)
+        opts = make_opts(order, use_graph=graph, tile=tile)
         st = lib().bcc_check_device(self._h, ROBOTS[robot], ctypes.c_void_p(d_edges_ptr), num_edges,
                                     resolution, ctypes.c_void_p(d_results_ptr), ctypes.byref(opts),
                                     ctypes.c_void_p(stream))

@@ -186,15 +186,20 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     a.max_prims = std::max(ctx->max_prims, 1);
     a.blob_smem = ctx->blob_smem;
     a.d_results = d_results;
-    // Tile: warps per CTA limited by shared memory; edges per CTA.
-    int warps = 8;
+    // Tile: warps per CTA (tuned, limited by shared memory); edges per CTA.
+    int warps = ctx->tune.warps;
     while (warps > 1 && bcc::check_smem_bytes(a.max_prims, a.blob_smem, warps) > 200 * 1024) warps >>= 1;
     if (bcc::check_smem_bytes(a.max_prims, a.blob_smem, warps) > 220 * 1024)
         return fail(ctx, BCC_ERR_LIMIT, "an environment has too many primitives for shared-memory staging");
     a.warps = warps;
-    a.edges_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : 128, 1, 1 << 20);
+    a.edges_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : ctx->tune.edges_per_cta, 1,
+                                 1 << 20);
     if ((E + a.edges_per_cta - 1) / a.edges_per_cta > 65535)
         a.edges_per_cta = (E + 65534) / 65535;
+    a.persistent = ctx->tune.persistent;
+    a.queue_min_items = ctx->tune.queue_min_items;
+    BCC_CUDA(ctx, ctx->work_counter.ensure(64));
+    a.work_counter = ctx->work_counter.as<int>();
     return BCC_OK;
 }
 
@@ -213,16 +218,14 @@ constexpr int kLearnedRowCap = 16 << 20;  // MLP rows per learned check (1.5 GB 
 // Learned order: (1) plain probe of each pair's first chunk, undecided pairs
 // queued with MLP rows for their segments; (2) segment features and tcgen05
 // MLP scores; (3) the queued pairs walked in descending segment score.
-bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
-    if (!ctx->mlp.ready) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned order needs MLP parameters (bcc_mlp_train or bcc_mlp_set_params)");
-    bcc_status s = ensure_env_code(ctx, st);
-    if (s != BCC_OK) return s;
+// Buffers are sized here, outside any stream capture.
+bcc_status prepare_learned(bcc_ctx* ctx, bcc::PipelineArgs& a) {
     const int grid = bcc::check_grid_size(a);
     const size_t qn = (size_t)grid * a.edges_per_cta;
     BCC_CUDA(ctx, ctx->q_count.ensure(sizeof(int) * (size_t)grid + 64));
     BCC_CUDA(ctx, ctx->q_edges.ensure(sizeof(int) * qn));
     BCC_CUDA(ctx, ctx->q_rows.ensure(sizeof(int) * qn));
-    long long cap_ll = (long long)a.num_envs * (a.total_rows / bcc::kSegment) + 64;
+    const long long cap_ll = (long long)a.num_envs * (a.total_rows / bcc::kSegment) + 64;
     const int cap = (int)std::min<long long>(cap_ll, kLearnedRowCap);
     BCC_CUDA(ctx, ctx->mlp.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)cap));
     BCC_CUDA(ctx, ctx->mlp.logits.ensure(sizeof(float) * (size_t)cap));
@@ -232,7 +235,14 @@ bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
     a.q_rows = ctx->q_rows.as<int>();
     a.row_cap = cap;
     a.logits = ctx->mlp.logits.as<float>();
-    a.queue_min_items = ctx->queue_min_items;
+    a.queue_min_items = ctx->tune.queue_min_items;
+    ctx->learned_rows_dev = a.row_count;
+    ctx->learned_row_cap = cap;
+    return BCC_OK;
+}
+
+bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
+    const int grid = bcc::check_grid_size(a);
     BCC_CUDA(ctx, cudaMemsetAsync(a.q_count, 0, sizeof(int) * ((size_t)grid + 1), st));
     cudaEvent_t* ev = a.stage_events;
     if (ev) cudaEventRecord(ev[1], st);
@@ -244,24 +254,30 @@ bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
     }
     a.mode = 1;
     BCC_CUDA(ctx, bcc::launch_check_mode(BCC_ROBOT_PANDA, a, st));
-    int rows = 0;
-    BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.row_count, sizeof(int), cudaMemcpyDeviceToHost, st));
-    BCC_CUDA(ctx, cudaStreamSynchronize(st));
-    rows = std::min(*ctx->h_total, cap);
-    ctx->last_learned_rows = rows;
-    if (rows > 0) {
-        BCC_CUDA(ctx, bcc::launch_queue_features(BCC_ROBOT_PANDA, a, ctx->env_code.as<float>(),
-                                                 ctx->mlp.x.as<uint16_t>(), grid, st));
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        BCC_CUDA(ctx, bcc::mlp_forward(ctx->mlp.x.as<uint16_t>(), rows, ctx->mlp.images.as<uint8_t>(),
-                                       ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
-                                       std::max(sms, 1), st));
-    }
+    // No host round trip: the feature kernel reads the queue and the MLP
+    // kernel reads the device row count (capped by the buffer capacity).
+    BCC_CUDA(ctx, bcc::launch_queue_features(BCC_ROBOT_PANDA, a, ctx->env_code.as<float>(), ctx->mlp.x.as<uint16_t>(),
+                                             grid, st));
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    BCC_CUDA(ctx, bcc::mlp_forward(ctx->mlp.x.as<uint16_t>(), a.row_cap, ctx->mlp.images.as<uint8_t>(),
+                                   ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
+                                   std::max(sms, 1), st, a.row_count));
     a.mode = 2;
     BCC_CUDA(ctx, bcc::launch_check_mode(BCC_ROBOT_PANDA, a, st));
     if (ev) cudaEventRecord(ev[5], st);
     return BCC_OK;
+}
+
+bcc_status launch_sequence(bcc_ctx* ctx, bcc_robot robot, bcc::PipelineArgs& a, bool learned, cudaStream_t st) {
+    if (learned) return run_learned(ctx, a, st);
+    BCC_CUDA(ctx, bcc::launch_check((int)robot, a, st));
+    return BCC_OK;
+}
+
+bool same_tune(const bcc::Tune& x, const bcc::Tune& y) {
+    return x.edges_per_cta == y.edges_per_cta && x.warps == y.warps && x.persistent == y.persistent &&
+           x.queue_min_items == y.queue_min_items;
 }
 
 bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution,
@@ -269,8 +285,57 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     bcc::PipelineArgs a;
     bcc_status s = prepare(ctx, robot, d_edges, E, resolution, d_results, opts, st, a);
     if (s != BCC_OK) return s;
-    if (opts && opts->order == BCC_ORDER_LEARNED) return run_learned(ctx, a, st);
-    BCC_CUDA(ctx, bcc::launch_check((int)robot, a, st));
+    const bool learned = opts && opts->order == BCC_ORDER_LEARNED;
+    if (learned) {
+        if (!ctx->mlp.ready)
+            return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned order needs MLP parameters (bcc_mlp_train or bcc_mlp_set_params)");
+        s = ensure_env_code(ctx, st);
+        if (s != BCC_OK) return s;
+        s = prepare_learned(ctx, a);
+        if (s != BCC_OK) return s;
+    }
+    const bool graph = opts && opts->use_graph && !ctx->counting && !(opts->tile_override > 0);
+    if (!graph) return launch_sequence(ctx, robot, a, learned, st);
+    // CUDA graph of everything after the discretisation (whose sample total sizes
+    // the launches): replayed while the inputs and configuration are unchanged.
+    bcc::GraphCache& G = ctx->graph[learned ? 1 : 0];
+    const bool hit = G.exec && G.edges == d_edges && G.results == d_results && G.stream == st && G.num_edges == E &&
+                     G.resolution == resolution && G.total_rows == a.total_rows && G.robot == (int)robot &&
+                     G.env_version == ctx->env_version && same_tune(G.tune, ctx->tune);
+    if (!hit) {
+        if (G.exec) {
+            cudaGraphExecDestroy(G.exec);
+            G.exec = nullptr;
+        }
+        a.stage_events = nullptr;
+        cudaGraph_t g = nullptr;
+        BCC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        s = launch_sequence(ctx, robot, a, learned, st);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (s != BCC_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
+        ce = cudaGraphInstantiate(&G.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaGraphInstantiate");
+        G.edges = d_edges;
+        G.results = d_results;
+        G.stream = st;
+        G.num_edges = E;
+        G.resolution = resolution;
+        G.total_rows = a.total_rows;
+        G.robot = (int)robot;
+        G.env_version = ctx->env_version;
+        G.tune = ctx->tune;
+    }
+    cudaEvent_t* ev = ctx->profiling ? ctx->ev : nullptr;
+    if (ev) cudaEventRecord(ev[1], st);
+    BCC_CUDA(ctx, cudaGraphLaunch(G.exec, st));
+    if (ev) {
+        for (int i = 2; i <= 5; ++i) cudaEventRecord(ev[i], st);
+    }
     return BCC_OK;
 }
 
@@ -528,6 +593,7 @@ bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
     ctx->max_prims = max_prims;
     ctx->blob_smem = blob_smem;
     ctx->env_code_ready = false;
+    ctx->env_version += 1;
     return BCC_OK;
 }
 
@@ -676,6 +742,114 @@ bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, i
     return BCC_OK;
 }
 
-int64_t bcc_last_learned_rows(const bcc_ctx* ctx) { return ctx ? ctx->last_learned_rows : -1; }
+int64_t bcc_last_learned_rows(const bcc_ctx* ctx) {
+    if (!ctx || !ctx->learned_rows_dev) return -1;
+    int rows = 0;
+    if (cudaMemcpy(&rows, ctx->learned_rows_dev, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return std::min(rows, ctx->learned_row_cap);
+}
+
+// Launch configuration: [0] edges per CTA, [1] warps per CTA, [2] persistent
+// kernel (0/1), [3] learned-order queue threshold (items).
+bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg) {
+    if (!ctx || !cfg) return BCC_ERR_INVALID_ARGUMENT;
+    cfg[0] = ctx->tune.edges_per_cta;
+    cfg[1] = ctx->tune.warps;
+    cfg[2] = ctx->tune.persistent;
+    cfg[3] = ctx->tune.queue_min_items;
+    return BCC_OK;
+}
+
+bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg) {
+    if (!ctx || !cfg) return BCC_ERR_INVALID_ARGUMENT;
+    if (cfg[0] < 1 || cfg[0] > 4096 || (cfg[1] != 1 && cfg[1] != 2 && cfg[1] != 4 && cfg[1] != 8) ||
+        (cfg[2] != 0 && cfg[2] != 1) || cfg[3] < 0)
+        return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad launch configuration");
+    ctx->tune.edges_per_cta = cfg[0];
+    ctx->tune.warps = cfg[1];
+    ctx->tune.persistent = cfg[2];
+    ctx->tune.queue_min_items = cfg[3];
+    return BCC_OK;
+}
+
+// Time each candidate configuration on the given edges against the uploaded
+// environments (1 warm-up + 3 timed checks, CUDA events) and keep the fastest.
+bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                        int32_t order, int32_t* chosen) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs <= 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    const int dof = bcc_robot_dof(robot);
+    if (!edges || num_edges <= 0 || dof < 0 || resolution <= 0) return BCC_ERR_INVALID_ARGUMENT;
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t eb = sizeof(float) * 2 * (size_t)dof * num_edges;
+    BCC_CUDA(ctx, ctx->edges.ensure(eb));
+    BCC_CUDA(ctx, ctx->results.ensure((size_t)num_edges * ctx->num_envs));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->edges.p, edges, eb, cudaMemcpyHostToDevice));
+    bcc_opts opts{};
+    opts.order = order;
+    cudaEvent_t e0, e1;
+    BCC_CUDA(ctx, cudaEventCreate(&e0));
+    BCC_CUDA(ctx, cudaEventCreate(&e1));
+    const bool saved_prof = ctx->profiling;
+    ctx->profiling = false;
+    auto time_cfg = [&](const bcc::Tune& t, float& ms) -> bcc_status {
+        ctx->tune = t;
+        bcc_status s = run_check(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, ctx->results.as<uint8_t>(),
+                                 &opts, st);
+        if (s != BCC_OK) return s;
+        BCC_CUDA(ctx, cudaEventRecord(e0, st));
+        for (int r = 0; r < 3; ++r) {
+            s = run_check(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, ctx->results.as<uint8_t>(), &opts,
+                          st);
+            if (s != BCC_OK) return s;
+        }
+        BCC_CUDA(ctx, cudaEventRecord(e1, st));
+        BCC_CUDA(ctx, cudaEventSynchronize(e1));
+        BCC_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+        return BCC_OK;
+    };
+    bcc::Tune best = ctx->tune;
+    float best_ms = 1e30f;
+    bcc_status s = BCC_OK;
+    const int tiles[4] = {32, 64, 128, 256};
+    const int warps[2] = {4, 8};
+    for (int ti = 0; ti < 4 && s == BCC_OK; ++ti)
+        for (int wi = 0; wi < 2 && s == BCC_OK; ++wi)
+            for (int pe = 0; pe < 2 && s == BCC_OK; ++pe) {
+                bcc::Tune t = best;
+                t.edges_per_cta = tiles[ti];
+                t.warps = warps[wi];
+                t.persistent = pe;
+                float ms = 0;
+                s = time_cfg(t, ms);
+                if (s == BCC_OK && ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+            }
+    if (s == BCC_OK && order == BCC_ORDER_LEARNED && ctx->mlp.ready) {
+        const int qmins[5] = {32, 64, 128, 256, 512};
+        bcc::Tune base = best;
+        for (int qi = 0; qi < 5 && s == BCC_OK; ++qi) {
+            bcc::Tune t = base;
+            t.queue_min_items = qmins[qi];
+            float ms = 0;
+            s = time_cfg(t, ms);
+            if (s == BCC_OK && ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->profiling = saved_prof;
+    best.tuned = true;
+    ctx->tune = best;
+    if (s != BCC_OK) return s;
+    if (chosen) bcc_get_launch_config(ctx, chosen);
+    return BCC_OK;
+}
 
 }  // extern "C"

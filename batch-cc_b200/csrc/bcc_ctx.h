@@ -42,6 +42,30 @@ struct MlpState {
     long long step = 0;      // Adam step count
 };
 
+// Launch configuration of the environment check (set by bcc_autotune).
+struct Tune {
+    int edges_per_cta = 128;
+    int warps = 8;
+    int persistent = 1;
+    int queue_min_items = 128;
+    bool tuned = false;
+};
+
+// A captured launch sequence (everything after the discretisation) and the
+// inputs it was captured for.
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    const void* edges = nullptr;
+    void* results = nullptr;
+    cudaStream_t stream = nullptr;
+    int num_edges = -1, resolution = -1, total_rows = -1, order = -1, robot = -1;
+    long long env_version = -1;
+    Tune tune;
+    ~GraphCache() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
 }  // namespace bcc
 
 struct bcc_ctx {
@@ -66,6 +90,10 @@ struct bcc_ctx {
     bcc::DevBuf env_code;    // [num_envs][32] environment encodings
     bool env_code_ready = false;
     bcc::DevBuf q_count, q_edges, q_rows;  // learned-order queue of undecided pairs
-    long long last_learned_rows = 0;       // MLP rows scored by the last learned check
-    int queue_min_items = 128;             // learned order: remaining items that justify scoring
+    const int* learned_rows_dev = nullptr; // device row count of the last learned check
+    int learned_row_cap = 0;
+    bcc::Tune tune;                        // launch configuration (autotuned or default)
+    bcc::DevBuf work_counter;              // persistent-kernel work queue head
+    long long env_version = 0;             // bumped by every upload (graph cache key)
+    bcc::GraphCache graph[2];              // per order (plain, learned)
 };

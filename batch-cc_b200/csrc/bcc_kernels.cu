@@ -20,6 +20,7 @@
 //                          (primitive, link) pairs are compacted, and the warp walks
 //                          (sample, pair) items 32 at a time in check order with a
 //                          warp-ballot exit on the first hit.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -269,49 +270,25 @@ __device__ __forceinline__ int slab_tri(float lo, float hi, float g0, float inv)
 // order, first 32-item chunk only; a pair still undecided after it is queued
 // (with MLP rows for its segments) instead of getting a verdict.  MODE 2
 // (phase 3): the CTA's queued pairs, walked in descending segment score.
+//
+// check_tile processes the edges of one (environment, edge tile) work item
+// with the environment's blob already staged in shared memory; it is shared
+// by the one-CTA-per-item grid kernel and the persistent kernel.
 template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
+__device__ __forceinline__ void check_tile(const CheckParams& P, int env, int tile, int n_slots,
+                                           const unsigned char* smem, uint8_t (*s_perm)[kMaxSegments], float4 h0,
+                                           float4 h1) {
     constexpr int G = M::num_env_groups;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
-
-    const int env = blockIdx.x;
-    const int e_begin = blockIdx.y * P.edges_per_cta;
-    const int e_end = min(e_begin + P.edges_per_cta, P.num_edges);
+    const int e_begin = tile * P.edges_per_cta;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cta = blockIdx.y * gridDim.x + blockIdx.x;
-    const int n_slots = MODE == 2 ? P.q_count[cta] : e_end - e_begin;
-    if (n_slots <= 0) return;
-
-    // Environment header: grid origin, inverse slab width, blob offset and shape.
-    const float4 h0 = P.env_hdr[2 * env + 0];
-    const float4 h1 = P.env_hdr[2 * env + 1];
-    const uint32_t blob_off = __float_as_uint(h0.w);
+    const int cta = tile * P.num_envs + env;
     const uint32_t shape = __float_as_uint(h1.w);
     const int np = (int)(shape & 0xffffu);
     const int W = (int)(shape >> 16);  // 64-bit words per primitive mask
-    const uint32_t blob_bytes = (uint32_t)np * kPrimF4 * 16u + 3u * kGridTri * (uint32_t)W * 8u;
-
     const float4* prim = reinterpret_cast<const float4*>(smem);
     const uint64_t* masks = reinterpret_cast<const uint64_t*>(smem + (size_t)np * kPrimF4 * 16);
-    uint16_t* pairs = reinterpret_cast<uint16_t*>(smem + P.blob_smem) + (size_t)warp * P.pairs_per_warp;
-
-    bool ok = true;
-    if (np > 0) {
-        if (threadIdx.x == 0) {
-            mbar_init(&bar, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)blob_off, blob_bytes, &bar);
-        ok = mbar_wait_bounded(&bar, 0u, 1u << 22);
-        if (!ok) {
-            if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
-            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
-            return;
-        }
-    }
+    uint16_t* pairs = reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) +
+                      (size_t)warp * P.pairs_per_warp;
     const DevTables<M>& T = tab<M>();
 
     for (int slot = warp; slot < n_slots; slot += WARPS) {
@@ -485,6 +462,101 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
     }
 }
 
+__device__ __forceinline__ int tile_slots(const CheckParams& P, int env, int tile, int mode) {
+    if (mode == 2) return P.q_count[tile * P.num_envs + env];
+    const int e_begin = tile * P.edges_per_cta;
+    return min(P.edges_per_cta, P.num_edges - e_begin);
+}
+
+__device__ __forceinline__ uint32_t blob_bytes_of(float4 h1) {
+    const uint32_t shape = __float_as_uint(h1.w);
+    return (shape & 0xffffu) * kPrimF4 * 16u + 3u * kGridTri * (shape >> 16) * 8u;
+}
+
+// One CTA per (environment, edge tile): blockIdx.x = environment, blockIdx.y = tile.
+template <class M, int WARPS, int MODE>
+__global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
+    const int env = blockIdx.x, tile = blockIdx.y;
+    const int n_slots = tile_slots(P, env, tile, MODE);
+    if (n_slots <= 0) return;
+    const float4 h0 = P.env_hdr[2 * env + 0];
+    const float4 h1 = P.env_hdr[2 * env + 1];
+    const uint32_t bytes = blob_bytes_of(h1);
+    if (bytes) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)__float_as_uint(h0.w), bytes, &bar);
+        if (!mbar_wait_bounded(&bar, 0u, 1u << 22)) {
+            if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
+            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
+            return;
+        }
+    }
+    check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, s_perm, h0, h1);
+}
+
+// Persistent: a grid sized to the resident capacity pulls environment-major
+// work items (environment, edge tile) from an atomic counter, two at a time so
+// that consecutive items usually share the environment and its staged blob.
+constexpr int kItemsPerGrab = 2;
+
+template <class M, int WARPS, int MODE>
+__global__ void __launch_bounds__(WARPS * 32) check_persistent_kernel(CheckParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
+    __shared__ int s_item;
+    const int tiles = (P.num_edges + P.edges_per_cta - 1) / P.edges_per_cta;
+    const long long items = (long long)P.num_envs * tiles;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int staged = -1;
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(P.work_counter, kItemsPerGrab);
+        __syncthreads();
+        const int first = s_item;
+        __syncthreads();
+        if (first >= items) break;
+        bool failed = false;
+        for (int item = first; item < first + kItemsPerGrab && item < items; ++item) {
+            const int env = item / tiles, tile = item - (item / tiles) * tiles;
+            const int n_slots = tile_slots(P, env, tile, MODE);
+            if (n_slots <= 0) continue;
+            const float4 h0 = P.env_hdr[2 * env + 0];
+            const float4 h1 = P.env_hdr[2 * env + 1];
+            if (env != staged) {
+                const uint32_t bytes = blob_bytes_of(h1);
+                __syncthreads();  // every warp is done with the previous blob
+                if (bytes) {
+                    if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)__float_as_uint(h0.w), bytes, &bar);
+                    const bool ok = mbar_wait_bounded(&bar, phase, 1u << 22);
+                    if (__syncthreads_or(!ok)) {
+                        if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
+                        mbar_wait_bounded(&bar, phase, 1u << 22);
+                        failed = true;
+                        break;
+                    }
+                    phase ^= 1u;
+                }
+                staged = env;
+            }
+            check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, s_perm, h0, h1);
+        }
+        if (failed) break;
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ launchers
 size_t check_smem_bytes(int max_prims, size_t blob_smem, int warps) {
     const size_t ppw = (size_t)((max_prims * 16 + 7) & ~7);
@@ -504,6 +576,23 @@ template <class M, int W, int MODE>
 static cudaError_t launch_check_wm(CheckParams P, int E, cudaStream_t st) {
     P.pairs_per_warp = (P.max_prims * M::num_env_groups + 7) & ~7;
     const size_t smem = P.blob_smem + (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
+    if (P.persistent) {
+        cudaError_t err = cudaFuncSetAttribute(check_persistent_kernel<M, W, MODE>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err != cudaSuccess) return err;
+        int per_sm = 0, dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, check_persistent_kernel<M, W, MODE>, W * 32, smem);
+        if (err != cudaSuccess) return err;
+        const long long items = (long long)P.num_envs * ((E + P.edges_per_cta - 1) / P.edges_per_cta);
+        long long grid = (long long)std::max(per_sm, 1) * std::max(sms, 1);
+        grid = std::min(grid, (items + kItemsPerGrab - 1) / kItemsPerGrab);
+        err = cudaMemsetAsync(P.work_counter, 0, sizeof(int), st);
+        if (err != cudaSuccess) return err;
+        check_persistent_kernel<M, W, MODE><<<(unsigned)std::max(grid, 1ll), W * 32, smem, st>>>(P);
+        return cudaGetLastError();
+    }
     cudaError_t err = cudaFuncSetAttribute(check_kernel<M, W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
     if (err != cudaSuccess) return err;
@@ -560,6 +649,9 @@ static cudaError_t run_check(const PipelineArgs& a, cudaStream_t st) {
     P.row_count = a.row_count;
     P.row_cap = a.row_cap;
     P.logits = a.logits;
+    P.queue_min_items = a.queue_min_items;
+    P.persistent = a.persistent;
+    P.work_counter = a.work_counter;
     switch (a.warps) {
         case 8: err = launch_check_w<M, 8>(P, E, st, a.mode); break;
         case 4: err = launch_check_w<M, 4>(P, E, st, a.mode); break;
@@ -787,6 +879,8 @@ static CheckParams params_of(const PipelineArgs& a) {
     P.logits = a.logits;
     P.counters = a.counters;
     P.queue_min_items = a.queue_min_items;
+    P.persistent = a.persistent;
+    P.work_counter = a.work_counter;
     return P;
 }
 

@@ -43,6 +43,8 @@ struct CheckParams {
     int row_cap;             // capacity of the MLP row buffers
     const float* logits;     // [row_cap] segment scores (mode 2)
     int queue_min_items;     // probe: queue only pairs with at least this many items left
+    int persistent;          // 1: persistent kernel pulling work items from work_counter
+    int* work_counter;
 };
 
 // Samples per learned-order segment: the MLP scores each run of 8 consecutive
@@ -85,6 +87,8 @@ struct PipelineArgs {
     int row_cap;
     const float* logits;
     int queue_min_items;
+    int persistent;
+    int* work_counter;
 };
 
 cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st);

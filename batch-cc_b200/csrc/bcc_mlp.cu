@@ -96,8 +96,11 @@ __device__ __forceinline__ void epilogue_relu_to_smem(uint32_t taddr, const floa
 // Persistent: each CTA (4 warps, one row per thread) loads the weights once and
 // runs 128-row tiles.  x: BF16 [rows][48] row-major; logits: FP32 [rows].
 __global__ void __launch_bounds__(128, 1)
-    mlp_forward_kernel(const uint16_t* __restrict__ x, int rows, const uint4* __restrict__ images,
-                       const float* __restrict__ params, float* __restrict__ logits, int* __restrict__ err) {
+    mlp_forward_kernel(const uint16_t* __restrict__ x, int rows, const int* __restrict__ rows_dev,
+                       const uint4* __restrict__ images, const float* __restrict__ params, float* __restrict__ logits,
+                       int* __restrict__ err) {
+    // rows_dev (optional): the row count produced on the device, capped by rows.
+    if (rows_dev) rows = min(rows, *rows_dev);
     extern __shared__ __align__(1024) uint8_t sm[];
     const int t = threadIdx.x, warp = t >> 5;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar);
@@ -501,14 +504,14 @@ cudaError_t mlp_pack(const float* d_params, uint8_t* d_images, cudaStream_t st) 
 }
 
 cudaError_t mlp_forward(const uint16_t* d_x, int rows, const uint8_t* d_images, const float* d_params,
-                        float* d_logits, int* d_err, int num_sms, cudaStream_t st) {
+                        float* d_logits, int* d_err, int num_sms, cudaStream_t st, const int* d_rows) {
     if (rows <= 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
     if (e != cudaSuccess) return e;
     const int tiles = (rows + 127) / 128;
     const int grid = tiles < num_sms ? tiles : num_sms;
-    mlp_forward_kernel<<<grid, 128, kFwdSmem, st>>>(d_x, rows, reinterpret_cast<const uint4*>(d_images), d_params,
-                                                     d_logits, d_err);
+    mlp_forward_kernel<<<grid, 128, kFwdSmem, st>>>(d_x, rows, d_rows, reinterpret_cast<const uint4*>(d_images),
+                                                     d_params, d_logits, d_err);
     return cudaGetLastError();
 }
 

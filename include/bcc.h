@@ -221,6 +221,25 @@ bcc_status bcc_mlp_train_step(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t*
  * short probe kernel (the roofline denominator of the scalar-FP32 checker). */
 bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
 
+/*
+ * Launch configuration of the environment check: cfg[0] edges per CTA, cfg[1]
+ * warps per CTA (1, 2, 4, 8; lowered automatically when an environment's
+ * shared-memory footprint needs it), cfg[2] 1 = persistent kernel pulling
+ * (environment, edge tile) work items from an atomic queue, 0 = one CTA per
+ * item, cfg[3] learned order: a pair is scored by the MLP only when at least
+ * this many (sample, pair) items remain after its first chunk.
+ */
+bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg);
+bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg);
+/*
+ * Autotuner: times candidate configurations (edges per CTA 32..256, 4 or 8
+ * warps, persistent or not, and for the learned order the queue threshold) on
+ * the given host edges against the uploaded environments and keeps the fastest
+ * in the context; chosen[4] receives it (may be NULL).  order: bcc_order.
+ */
+bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
+                        int32_t order, int32_t* chosen);
+
 /* Number of samples the reference discretisation checks for one edge
  * (32 * max(ceil(|end - start|_2 / 31 * resolution), 1), src/batch_cc.cu:103-116). */
 int32_t bcc_edge_samples(const float* start, const float* end, int32_t dof, int32_t resolution);
