@@ -299,7 +299,7 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     // CUDA graph of everything after the discretisation (whose sample total sizes
     // the launches): replayed while the inputs and configuration are unchanged.
     bcc::GraphCache& G = ctx->graph[learned ? 1 : 0];
-    const bool hit = G.exec && G.edges == d_edges && G.results == d_results && G.stream == st && G.num_edges == E &&
+    const bool hit = G.exec && G.edges == d_edges && G.results == d_results && G.num_edges == E &&
                      G.resolution == resolution && G.total_rows == a.total_rows && G.robot == (int)robot &&
                      G.env_version == ctx->env_version && same_tune(G.tune, ctx->tune);
     if (!hit) {
@@ -309,9 +309,12 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
         }
         a.stage_events = nullptr;
         cudaGraph_t g = nullptr;
-        BCC_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        s = launch_sequence(ctx, robot, a, learned, st);
-        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        // Captured on the context's private stream (the caller's may be the legacy
+        // default stream, which cannot be captured); launched on the caller's.
+        cudaStream_t cs = ctx->capture_stream;
+        BCC_CUDA(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        s = launch_sequence(ctx, robot, a, learned, cs);
+        cudaError_t ce = cudaStreamEndCapture(cs, &g);
         if (s != BCC_OK) {
             if (g) cudaGraphDestroy(g);
             return s;
@@ -350,6 +353,7 @@ bcc_status bcc_create(bcc_ctx** out, int device) {
     c->device = device;
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->capture_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_total, sizeof(int));
     if (e != cudaSuccess) {
         delete c;
@@ -366,7 +370,13 @@ void bcc_destroy(bcc_ctx* ctx) {
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->h_total) cudaFreeHost(ctx->h_total);
+    for (auto& g : ctx->graph)
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->capture_stream) cudaStreamDestroy(ctx->capture_stream);
     delete ctx;
 }
 

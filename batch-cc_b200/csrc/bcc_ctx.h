@@ -71,6 +71,7 @@ struct GraphCache {
 struct bcc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t capture_stream = nullptr;  // private stream for CUDA-graph capture
     std::string err;
     bool tables[3] = {false, false, false};
     // environment arena
