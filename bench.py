@@ -227,28 +227,36 @@ def train_proposal(chk, args):
 
 
 def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev):
+    """Timed region: `steps` graph-captured (persistent-kernel) checks, L2 flushed
+    between steps outside the timed events; then an untimed eager pass for the
+    per-stage breakdown."""
     import torch
 
-    def step():
-        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream)
+    def step(graph):
+        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream, graph=graph)
 
     for _ in range(warmup):
-        step()
+        step(True)
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    stage_tot, check_ms = {}, []
     for i in range(steps):
         flush.fill_(float(i))  # evict L2 between timed iterations (untimed)
         evs[i][0].record(stream)
-        step()
+        step(True)
         evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    total_ms = sum(x.elapsed_time(y) for x, y in evs)
+    stage_tot, check_ms = {}, []
+    reps = 3
+    for i in range(reps):
+        flush.fill_(float(i))
+        step(False)
         torch.cuda.synchronize()
         st = chk.stage_times()
         check_ms.append(st["check"])
         for k, v in st.items():
             stage_tot[k] = stage_tot.get(k, 0.0) + v
-    total_ms = sum(x.elapsed_time(y) for x, y in evs)
-    return total_ms, check_ms, {k: v / steps for k, v in stage_tot.items()}
+    return total_ms, check_ms, {k: v / reps for k, v in stage_tot.items()}
 
 
 def mlp_roofline(chk, dev, rows=1 << 22, reps=5):
@@ -292,12 +300,15 @@ def run_ours(args, world, rank, local, dist):
     d_res2 = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
+    # Autotuned launch configuration per order (untimed), on the first edges.
+    tuned = {o: chk.autotune(edges[:min(E, 2000)], order=o) for o in ("plain", "learned")}
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     results = {}
     with ClockSampler(dev) as clk:
         for order in ("plain", "learned"):
+            chk.set_launch_config(**tuned[order])
             results[order] = time_order(chk, d_edges, d_res, E, order, stream, args.steps, args.warmup, flush, dev)
     torch.cuda.synchronize()
 
@@ -313,13 +324,16 @@ def run_ours(args, world, rank, local, dist):
     value = world * N * E / (ms[head] * 1e-3)
 
     # Verdict agreement of the two orders (must be identical), and work counters.
+    chk.set_launch_config(**tuned["plain"])
     chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="plain", stream=stream.cuda_stream)
+    chk.set_launch_config(**tuned["learned"])
     chk.check_device(d_edges.data_ptr(), E, d_res2.data_ptr(), order="learned", stream=stream.cuda_stream)
     torch.cuda.synchronize()
     mismatch = int((d_res != d_res2).sum().item())
     work = {}
     chk.set_profiling(True, counters=True)
     for order in ("plain", "learned"):
+        chk.set_launch_config(**tuned[order])
         chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream)
         torch.cuda.synchronize()
         c = chk.work_counters()
@@ -333,6 +347,7 @@ def run_ours(args, world, rank, local, dist):
     # e2e: the public host API (pinned host edges in, verdicts out), per step.
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
     h_res = torch.empty((E, N), dtype=torch.uint8).pin_memory().numpy()
+    chk.set_launch_config(**tuned[head])
     chk.check(h_edges, out=h_res, order=head)
     t_e2e = []
     for _ in range(max(3, min(args.steps, 5))):
@@ -354,7 +369,8 @@ def run_ours(args, world, rank, local, dist):
                        "envs": N, "edges_per_gpu": E, "order": head,
                        "l2": "256 MB buffer written between timed steps (untimed)", "parallelism": "dp%d" % world},
             "orders": {o: {"value": world * N * E / (ms[o] * 1e-3), "ms_per_step": ms[o],
-                           "stages_ms_per_step": results[o][2], "work_per_pair": work[o]} for o in results},
+                           "launch": dict(tuned[o], graph=True), "stages_ms_per_step_eager": results[o][2],
+                           "work_per_pair": work[o]} for o in results},
             "learned_over_plain": ms["plain"] / ms["learned"],
             "verdict_mismatches_learned_vs_plain": mismatch,
             "proposal": dict(proposal, scored_segments_per_step=learned_rows),
