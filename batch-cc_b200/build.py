@@ -58,8 +58,23 @@ def build_lib(force=False):
     return LIB
 
 
+CXX = os.environ.get("CXX", "g++")
+CLI = os.path.join(HERE, "batch_cc")
+
+
+def build_cli(force=False):
+    """The drop-in command-line driver, linked against libbcc.so (rpath $ORIGIN)."""
+    srcs = glob.glob(os.path.join(HERE, "cli", "*")) + glob.glob(os.path.join(ROOT, "include", "src", "**", "*.hh"),
+                                                                  recursive=True) + [LIB]
+    if force or _newer(CLI, srcs):
+        _run([CXX, "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(HERE, "cli"),
+              os.path.join(HERE, "cli", "batch_cc.cpp"), "-o", CLI, "-L", HERE, "-lbcc", "-Wl,-rpath,$ORIGIN"])
+    return CLI
+
+
 def build_all(force=False):
     build_lib(force)
+    build_cli(force)
 
 
 if __name__ == "__main__":
