@@ -19,13 +19,23 @@ with numpy, and re-expresses the robot as data of this project's own format:
 * the gate/leaf structure of the environment and self checks, in the
   reference's order.
 
-The chain parameters are the public Franka Panda joint origins; the script
-verifies that the chain reproduces every sphere centre of the generated code
-to FP64 rounding over random configurations before writing anything.
+For Panda the chain parameters are the public Franka Panda joint origins; the
+script verifies that the chain reproduces every sphere centre of the generated
+code to FP64 rounding over random configurations before writing anything.
+
+Fetch (``fkcc<Fetch>``, ``src/utils.cuh:10382-24992``) and Baxter
+(``fkcc<Baxter>``, ``:24994-38241``) are generated in a different style (SSA
+``auto NAME = EXPR;`` statements, FK interleaved with the checks); for them
+the kinematic tree (revolute and prismatic joints, two arms for Baxter) is
+fitted to the evaluated expressions by ``fit_tree.py`` and verified the same
+way.  Baxter's generated FK composes quaternions whose constants carry seven
+digits (0.7071068, 0.9238792, ...), so it is rigid only to about 2e-7 m; the
+fitted tree reproduces it to that level.
 
 Usage (reads the reference tree; run in the development container only)::
 
-    python extract_robot.py <path-to-reference>/src/utils.cuh panda panda.json
+    python extract_robot.py <path-to-reference>/src/utils.cuh panda panda.json [golden.json]
+    python extract_robot.py <path-to-reference>/src/utils.cuh fetch fetch.json [golden.json]
 """
 import json
 import math
@@ -288,11 +298,141 @@ def extract_panda(utils_path):
     }
 
 
+SSA_DOF = {"fetch": 8, "baxter": 14}
+MAX_ENV_GROUPS = 32       # one lane per group in the checker's cull
+OVERHANG_EPS = 1e-6       # leaves sticking out less than this count as contained (m)
+CULL_PAD_MARGIN = 1e-5    # extra cull radius on top of the measured overhang (m)
+
+
+def extract_ssa(utils_path, robot):
+    """Fetch / Baxter: generated SSA code -> fitted kinematic tree + tables.
+
+    Check groups keep the reference's bound/leaf structure with three
+    adjustments the checker's table layout needs (none changes a verdict):
+    a group without leaves tests its bound sphere directly, so it gets that
+    sphere as its one leaf; a sphere used in several roles (bound of one
+    group, leaf of another) is duplicated so that every role has its own
+    sample-table row; and when there are more than 32 groups, leafless
+    groups on the same frame are merged under a synthetic bound that encloses
+    them (a leaf inside its bound needs no gate of its own)."""
+    import fit_tree
+
+    text = open(utils_path).read()
+    qname, body = _function_body(text, robot.capitalize())
+    stmts, env_raw, self_raw = fit_tree.parse_ssa(body)
+    dof = SSA_DOF[robot]
+    keys = []
+
+    def key(t):
+        if t not in keys:
+            keys.append(t)
+        return keys.index(t)
+
+    for g in env_raw:
+        key(g["bound"])
+        for l in g["leaves"]:
+            key(l)
+    for g in self_raw:
+        key(g["bound"][0])
+        key(g["bound"][1])
+        for a, b in g["pairs"]:
+            key(a)
+            key(b)
+    fk = fit_tree.make_evaluator(stmts, qname)
+    rng = np.random.default_rng(1234)
+    joints, body_of, base = fit_tree.fit_tree(fk, keys, dof, rng)
+    mj, frames, local = fit_tree.to_model(joints, body_of, base)
+
+    max_err = 0.0
+    for _ in range(2000):
+        q = rng.uniform(-4.0, 4.0, dof)
+        want = fit_tree.centres(fk, keys, q[None])[:, 0, :]
+        got = fit_tree.chain_centres(mj, frames, local, q)
+        max_err = max(max_err, float(np.abs(got - want).max()))
+    if max_err > 1e-6:
+        raise SystemExit("fitted tree does not reproduce the generated FK: max err %g" % max_err)
+
+    spheres = [{"frame": frames[i], "local": list(map(float, local[i])), "r": float(np.float32(float(k[3]))),
+                "link": None, "src": i} for i, k in enumerate(keys)]
+    used = set()
+
+    def role(i):
+        """Sphere index for a new table role of source sphere i (duplicated if taken)."""
+        if i not in used:
+            used.add(i)
+            return i
+        spheres.append(dict(spheres[i]))
+        return len(spheres) - 1
+
+    groups = [{"link": g["link"] or "unnamed", "bound": key(g["bound"]),
+               "leaves": [key(l) for l in g["leaves"]]} for g in env_raw]
+    if len(groups) > MAX_ENV_GROUPS:
+        by_frame = {}
+        for gi, g in enumerate(groups):
+            if not g["leaves"]:
+                by_frame.setdefault(frames[g["bound"]], []).append(gi)
+        merged, drop = [], set()
+        for f, gis in sorted(by_frame.items()):
+            if len(gis) < 2 or len(groups) - len(drop) <= MAX_ENV_GROUPS:
+                continue
+            mem = [groups[gi]["bound"] for gi in gis]
+            c, r = fit_tree.enclosing_sphere([local[m] for m in mem], [spheres[m]["r"] for m in mem])
+            r32 = float(np.nextafter(np.float32(r + 1e-6), np.float32(np.inf)))
+            spheres.append({"frame": f, "local": list(map(float, c)), "r": r32, "link": None, "src": -1})
+            merged.append({"link": "+".join(groups[gi]["link"] for gi in gis), "bound": len(spheres) - 1,
+                           "leaves": mem, "synthetic": True})
+            drop.update(gis)
+        groups = [g for gi, g in enumerate(groups) if gi not in drop] + merged
+    if len(groups) > MAX_ENV_GROUPS:
+        raise SystemExit("%d environment groups (max %d)" % (len(groups), MAX_ENV_GROUPS))
+
+    envs = []
+    for g in groups:
+        b_src = g["bound"]
+        leaves_src = g["leaves"] if g["leaves"] else [b_src]
+        b = role(b_src) if not g.get("synthetic") else b_src
+        # overhang of each leaf beyond the bound, max over all joint values
+        over = []
+        for l in leaves_src:
+            d = fit_tree.max_distance(mj, spheres[l]["frame"], np.array(spheres[l]["local"]),
+                                      spheres[b]["frame"], np.array(spheres[b]["local"]), dof)
+            over.append(d + spheres[l]["r"] - spheres[b]["r"])
+        order = sorted(range(len(leaves_src)), key=lambda i: (over[i] <= OVERHANG_EPS, i))
+        leaves = [role(leaves_src[i]) for i in order]
+        n_over = sum(1 for o in over if o > OVERHANG_EPS)
+        pad = max([0.0] + [o for o in over if o > OVERHANG_EPS])
+        pad = float(np.float32(pad + CULL_PAD_MARGIN)) if n_over else 0.0
+        for i in [b] + leaves:
+            spheres[i]["link"] = spheres[i]["link"] or g["link"]
+        envs.append({"link": g["link"], "bound": b, "leaves": leaves, "over_count": n_over, "cull_pad": pad,
+                     "max_overhang_m": max(over)})
+    selfs = []
+    for g in self_raw:
+        la, lb = g["links"] if g["links"] else ("?", "?")
+        pairs = [[key(a), key(b)] for a, b in g["pairs"]]
+        ba, bb = key(g["bound"][0]), key(g["bound"][1])
+        if not pairs:
+            pairs = [[ba, bb]]
+        selfs.append({"links": [la, lb], "bound": [ba, bb], "pairs": pairs})
+    for s in spheres:
+        s["link"] = s["link"] or "self_only"
+    return {
+        "robot": robot,
+        "dof": dof,
+        "fk_precision": 64,
+        "joints": mj,
+        "spheres": [{k: s[k] for k in ("frame", "local", "r", "link", "src")} for s in spheres],
+        "env_groups": envs,
+        "self_groups": selfs,
+        "fk_max_abs_err_vs_generated_code_m": max_err,
+        "_fk_eval": fk,
+        "_sphere_src": keys,
+    }
+
+
 def main():
     utils_path, robot, out = sys.argv[1], sys.argv[2], sys.argv[3]
-    if robot != "panda":
-        raise SystemExit("only panda is extracted by this script version")
-    model = extract_panda(utils_path)
+    model = extract_panda(utils_path) if robot == "panda" else extract_ssa(utils_path, robot)
     fk = model.pop("_fk_eval")
     src = model.pop("_sphere_src")
     # Golden FK vectors: sphere centres of the generated code (FP64) at seeded q.
@@ -300,23 +440,31 @@ def main():
     gold = []
     for _ in range(64):
         q = rng.uniform(-3.2, 3.9, model["dof"]).astype(np.float32).astype(np.float64)
-        vals = fk(q)
+        vals = fk(q) if robot == "panda" else {k: v[0] for k, v in fk(q[None]).items() if k != "q"}
         cs = []
         for k in src:
             cs.append([float(vals[t]) if not re.match(r"^-?[\d.]", t) else float(t) for t in k[:3]])
         gold.append({"q": q.tolist(), "centres": cs})
+    gold_doc = {"robot": robot, "cases": gold}
+    if robot != "panda":
+        # model sphere -> index into "centres" (-1: synthetic bound, no source)
+        gold_doc["src_of_sphere"] = [s["src"] for s in model["spheres"]]
     with open(out, "w") as f:
         json.dump(model, f, indent=1)
     if len(sys.argv) > 4:
         with open(sys.argv[4], "w") as f:
-            json.dump({"robot": robot, "cases": gold}, f)
+            json.dump(gold_doc, f)
     print("spheres=%d env_groups=%d self_groups=%d self_pairs=%d fk_err=%.3g" % (
         len(model["spheres"]), len(model["env_groups"]), len(model["self_groups"]),
         sum(len(g["pairs"]) for g in model["self_groups"]),
         model["fk_max_abs_err_vs_generated_code_m"]))
-    for c in model["containment"]:
+    for c in model.get("containment", []):
         if c["leaf_excess_m"] > 0:
             print("leaf outside bound:", c)
+    for g in model["env_groups"]:
+        if g.get("over_count"):
+            print("group %s: %d leaves overhang the bound by up to %.3g m" % (g["link"], g["over_count"],
+                                                                              g["max_overhang_m"]))
 
 
 if __name__ == "__main__":

@@ -1,6 +1,7 @@
 """Write the C++/CUDA robot-model header from an extracted robot JSON.
 
-The header holds plain constexpr tables (joint fixed transforms, sphere
+The header holds plain constexpr tables (joint fixed transforms, parents and
+types, sphere
 frames/offsets/radii, environment and self check groups, joint-limit scale)
 inside one struct per robot, usable from host C++ (the CPU oracle) and from
 CUDA device code (the checker kernels), where unrolled loops over the tables
@@ -21,7 +22,16 @@ import numpy as np
 LIMITS = {
     "panda": ([5.9342, 3.6652, 5.9342, 3.2289, 5.9342, 3.9095999999999997, 5.9342],
               [-2.9671, -1.8326, -2.9671, -3.1416, -2.9671, -0.0873, -2.9671]),
+    "fetch": ([0.38615, 3.2112, 2.739, 6.28318, 4.502, 6.28318, 4.32, 6.28318],
+              [0.0, -1.6056, -1.221, -3.14159, -2.251, -3.14159, -2.16, -3.14159]),
+    "baxter": ([3.40335987756, 3.194, 6.10835987756, 2.6679999999999997, 6.118, 3.66479632679, 6.118] * 2,
+               [-1.70167993878, -2.147, -3.05417993878, -0.05, -3.059, -1.57079632679, -3.059] * 2),
 }
+
+# Arithmetic operations of one generated FK evaluation (operators plus sin/cos
+# calls of the reference's straight-line FK statements): used for the
+# algorithmic FLOP count.
+FK_FLOPS = {"panda": 1150, "fetch": 983, "baxter": 1792}
 
 
 def rpy_matrix(r, p, y):
@@ -52,7 +62,7 @@ def main():
     lines = []
     w = lines.append
     w("// Generated by batch-cc_b200/robots/gen_header.py from %s.json -- do not edit." % name)
-    w("// Kinematic chain + collision-sphere tables of the %s robot, extracted from the" % name)
+    w("// Kinematic tree + collision-sphere tables of the %s robot, extracted from the" % name)
     w("// reference's generated fkcc<%s> (src/utils.cuh) and verified against it in FP64." % name.capitalize())
     w("#pragma once")
     w("")
@@ -66,16 +76,30 @@ def main():
     w("    static constexpr int num_self_groups = %d;" % len(slf))
     w("    static constexpr int num_self_pairs = %d;" % sum(len(g["pairs"]) for g in slf))
     w("")
-    w("    // Fixed transform of joint k (row-major 3x4: rotation | translation); the joint")
-    w("    // then rotates about its local z axis.  frame k+1 = frame k * F_k * Rz(q_k).")
+    w("    // FK arithmetic width of the reference's generated code for this robot")
+    w("    // (32: float expressions; 64: double expressions, centres rounded to float).")
+    w("    static constexpr int fk_precision = %d;" % m.get("fk_precision", 32))
+    w("    static constexpr int fk_flops = %d;" % FK_FLOPS[name])
+    w("")
+    w("    // Fixed transform of joint k (row-major 3x4: rotation | translation).")
+    w("    // frame k+1 = frame joint_parent[k] * F_k * J_k(q_k), J = Rz(q) for a revolute")
+    w("    // joint (type 0), Tz(q) for a prismatic one (type 1); frame 0 is the base.")
     w("    static constexpr double joint_tf[%d][12] = {" % dof)
-    for j in m["joints"]:
-        R = rpy_matrix(*j["rpy"])
-        t = j["xyz"]
-        vals = [R[0, 0], R[0, 1], R[0, 2], t[0], R[1, 0], R[1, 1], R[1, 2], t[1],
-                R[2, 0], R[2, 1], R[2, 2], t[2]]
+    parents, types = [], []
+    for k, j in enumerate(m["joints"]):
+        if "tf" in j:
+            vals = j["tf"]
+        else:
+            R = rpy_matrix(*j["rpy"])
+            t = j["xyz"]
+            vals = [R[0, 0], R[0, 1], R[0, 2], t[0], R[1, 0], R[1, 1], R[1, 2], t[1],
+                    R[2, 0], R[2, 1], R[2, 2], t[2]]
+        parents.append(j.get("parent_frame", k))
+        types.append(1 if j.get("type") == "prismatic" else 0)
         w("        {%s}," % ", ".join(fmt(v) for v in vals))
     w("    };")
+    w("    static constexpr int joint_parent[%d] = {%s};" % (dof, ", ".join(map(str, parents))))
+    w("    static constexpr int joint_type[%d] = {%s};" % (dof, ", ".join(map(str, types))))
     w("")
     w("    // Sphere k: chain frame (0 = base), offset in that frame (m), radius (m, float).")
     w("    static constexpr int sphere_frame[%d] = {%s};" % (
@@ -96,6 +120,13 @@ def main():
     w("    static constexpr int env_leaf_begin[%d] = {%s};" % (len(begins), ", ".join(map(str, begins))))
     w("    static constexpr int env_leaves[%d] = {%s};" % (
         begins[-1], ", ".join(str(i) for g in env for i in g["leaves"])))
+    w("    // Leaves of group g that may stick out of its bound (the first env_over_count[g]")
+    w("    // of the group's leaves) and the radius (m) the bound must grow by to contain")
+    w("    // every leaf at any joint value; 0 where all leaves lie inside the bound.")
+    w("    static constexpr int env_over_count[%d] = {%s};" % (
+        len(env), ", ".join(str(g.get("over_count", 0)) for g in env)))
+    w("    static constexpr float env_cull_pad[%d] = {%s};" % (
+        len(env), ", ".join(repr(float(np.float32(g.get("cull_pad", 0.0)))) + "f" for g in env)))
     w("")
     w("    // Self checks in reference order: group g gates on the bound pair self_bound[g]")
     w("    // and then tests the leaf pairs self_pairs[self_pair_begin[g] .. self_pair_begin[g+1]).")
@@ -115,6 +146,7 @@ def main():
     # env-checked leaves in env_leaves order, then every other sphere.
     order = [g["bound"] for g in env] + [i for g in env for i in g["leaves"]]
     order += [i for i in range(len(sph)) if i not in order]
+    assert len(set(order)) == len(order) == len(sph), "a sphere holds two table roles"
     pos = [0] * len(sph)
     for k, i in enumerate(order):
         pos[i] = k
