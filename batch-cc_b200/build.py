@@ -8,6 +8,7 @@ Every nvcc invocation targets `-gencode arch=compute_100a,code=sm_100a`; nvcc
 cross-compiles without a GPU.  Rebuilds only when a source is newer than the
 output.
 """
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -48,11 +49,16 @@ def build_lib(force=False):
     objs = []
     dep = deps()
     os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    jobs = []
     for src in sources():
         obj = os.path.join(HERE, "_build", os.path.basename(src) + ".o")
         if force or _newer(obj, dep):
-            _run([NVCC] + ARCH + NVFLAGS + ["-c", src, "-o", obj])
+            jobs.append([NVCC] + ARCH + NVFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
+    # one nvcc process per translation unit, run side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j) for j in jobs]:
+            f.result()
     if force or _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
     return LIB

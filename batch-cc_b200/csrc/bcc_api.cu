@@ -139,9 +139,12 @@ int clamp_tile(int v, int lo, int hi) { return std::max(lo, std::min(hi, v)); }
 bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution, uint8_t* d_results,
                    const bcc_opts* opts, cudaStream_t st, bcc::PipelineArgs& a) {
     const int r = (int)robot;
-    if (r != BCC_ROBOT_PANDA) return fail(ctx, BCC_ERR_NOT_SUPPORTED, "robot not built into this library");
+    const bcc::RobotOps* ops = bcc::robot_ops(r);
+    if (!ops) return fail(ctx, BCC_ERR_NOT_SUPPORTED, "robot not built into this library");
+    if (ctx->max_prims > ops->max_prims)
+        return fail(ctx, BCC_ERR_LIMIT, "an environment has more primitives than this robot's checker supports");
     if (!ctx->tables[r]) {
-        BCC_CUDA(ctx, bcc::upload_robot_tables(r));
+        BCC_CUDA(ctx, ops->upload_tables());
         ctx->tables[r] = true;
     }
     a = bcc::PipelineArgs{};
@@ -151,7 +154,7 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     BCC_CUDA(ctx, ctx->steps.ensure(sizeof(int) * (size_t)E));
     BCC_CUDA(ctx, ctx->offs.ensure(sizeof(int) * ((size_t)E + 1)));
     BCC_CUDA(ctx, ctx->edge_self.ensure(sizeof(int) * (size_t)E));
-    const int G = bcc::robot_num_env_groups(r);
+    const int G = ops->num_env_groups;
     BCC_CUDA(ctx, ctx->swept.ensure(sizeof(float4) * 2 * (size_t)G * E));
     BCC_CUDA(ctx, ctx->error_flag.ensure(sizeof(int)));
     a.steps = ctx->steps.as<int>();
@@ -167,14 +170,14 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
         BCC_CUDA(ctx, cudaMemsetAsync(a.counters, 0, sizeof(unsigned long long) * bcc::kNumCounters, st));
     }
     BCC_CUDA(ctx, cudaMemsetAsync(a.error_flag, 0, sizeof(int), st));
-    BCC_CUDA(ctx, bcc::launch_steps(r, a, st));
+    BCC_CUDA(ctx, ops->steps(a, st));
     BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.offs + E, sizeof(int), cudaMemcpyDeviceToHost, st));
     BCC_CUDA(ctx, cudaStreamSynchronize(st));
     const int total = *ctx->h_total;
     // offs[] is int32: the scan wraps past 2^31; cap the sample table at 2^27 rows.
     if (total < 0 || total > (1 << 27))
         return fail(ctx, BCC_ERR_LIMIT, "too many samples in one call (edges too long or non-finite)");
-    const int NS = bcc::robot_num_spheres(r);
+    const int NS = ops->num_spheres;
     BCC_CUDA(ctx, ctx->table.ensure(sizeof(float4) * (size_t)NS * std::max(total, 1)));
     BCC_CUDA(ctx, ctx->row_edge.ensure(sizeof(int) * (size_t)std::max(total, 1)));
     a.total_rows = total;
@@ -188,8 +191,8 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     a.d_results = d_results;
     // Tile: warps per CTA (tuned, limited by shared memory); edges per CTA.
     int warps = ctx->tune.warps;
-    while (warps > 1 && bcc::check_smem_bytes(a.max_prims, a.blob_smem, warps) > 200 * 1024) warps >>= 1;
-    if (bcc::check_smem_bytes(a.max_prims, a.blob_smem, warps) > 220 * 1024)
+    while (warps > 1 && bcc::check_smem_bytes(a.max_prims, G, a.blob_smem, warps) > 200 * 1024) warps >>= 1;
+    if (bcc::check_smem_bytes(a.max_prims, G, a.blob_smem, warps) > 220 * 1024)
         return fail(ctx, BCC_ERR_LIMIT, "an environment has too many primitives for shared-memory staging");
     a.warps = warps;
     a.edges_per_cta = clamp_tile(opts && opts->tile_override > 0 ? opts->tile_override : ctx->tune.edges_per_cta, 1,
@@ -206,7 +209,7 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
 // Environment codes of the uploaded set (once per upload).
 bcc_status ensure_env_code(bcc_ctx* ctx, cudaStream_t st) {
     if (ctx->env_code_ready) return BCC_OK;
-    BCC_CUDA(ctx, ctx->env_code.ensure(sizeof(float) * 32 * (size_t)std::max(ctx->num_envs, 1)));
+    BCC_CUDA(ctx, ctx->env_code.ensure(sizeof(float) * bcc::kEnvCode * (size_t)std::max(ctx->num_envs, 1)));
     BCC_CUDA(ctx, bcc::launch_env_encode(ctx->blobs.as<float4>(), ctx->env_hdr.as<float4>(), ctx->num_envs,
                                          ctx->env_code.as<float>(), st));
     ctx->env_code_ready = true;
@@ -241,37 +244,32 @@ bcc_status prepare_learned(bcc_ctx* ctx, bcc::PipelineArgs& a) {
     return BCC_OK;
 }
 
-bcc_status run_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, cudaStream_t st) {
+bcc_status run_learned(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::PipelineArgs& a, cudaStream_t st) {
     const int grid = bcc::check_grid_size(a);
     BCC_CUDA(ctx, cudaMemsetAsync(a.q_count, 0, sizeof(int) * ((size_t)grid + 1), st));
     cudaEvent_t* ev = a.stage_events;
-    if (ev) cudaEventRecord(ev[1], st);
-    BCC_CUDA(ctx, bcc::launch_prep(BCC_ROBOT_PANDA, a, st));
-    if (ev) {
-        cudaEventRecord(ev[2], st);
-        cudaEventRecord(ev[3], st);
-        cudaEventRecord(ev[4], st);
-    }
+    BCC_CUDA(ctx, ops->prep(a, st));  // records stage events 1-4
     a.mode = 1;
-    BCC_CUDA(ctx, bcc::launch_check_mode(BCC_ROBOT_PANDA, a, st));
+    BCC_CUDA(ctx, ops->check_mode(a, st));
     // No host round trip: the feature kernel reads the queue and the MLP
     // kernel reads the device row count (capped by the buffer capacity).
-    BCC_CUDA(ctx, bcc::launch_queue_features(BCC_ROBOT_PANDA, a, ctx->env_code.as<float>(), ctx->mlp.x.as<uint16_t>(),
-                                             grid, st));
+    BCC_CUDA(ctx, ops->queue_features(a, ctx->env_code.as<float>(), ctx->mlp.x.as<uint16_t>(), grid, st));
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     BCC_CUDA(ctx, bcc::mlp_forward(ctx->mlp.x.as<uint16_t>(), a.row_cap, ctx->mlp.images.as<uint8_t>(),
                                    ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
                                    std::max(sms, 1), st, a.row_count));
     a.mode = 2;
-    BCC_CUDA(ctx, bcc::launch_check_mode(BCC_ROBOT_PANDA, a, st));
+    BCC_CUDA(ctx, ops->check_mode(a, st));
     if (ev) cudaEventRecord(ev[5], st);
     return BCC_OK;
 }
 
 bcc_status launch_sequence(bcc_ctx* ctx, bcc_robot robot, bcc::PipelineArgs& a, bool learned, cudaStream_t st) {
-    if (learned) return run_learned(ctx, a, st);
-    BCC_CUDA(ctx, bcc::launch_check((int)robot, a, st));
+    const bcc::RobotOps* ops = bcc::robot_ops((int)robot);
+    if (!ops) return fail(ctx, BCC_ERR_NOT_SUPPORTED, "robot not built into this library");
+    if (learned) return run_learned(ctx, ops, a, st);
+    BCC_CUDA(ctx, ops->check(a, st));
     return BCC_OK;
 }
 
@@ -665,13 +663,13 @@ bcc_status bcc_mlp_train(bcc_ctx* ctx, bcc_robot robot, const float* edges, int3
     bcc::PipelineArgs a;
     bcc_status s = prepare(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, nullptr, nullptr, st, a);
     if (s != BCC_OK) return s;
-    BCC_CUDA(ctx, bcc::launch_prep((int)robot, a, st));
+    BCC_CUDA(ctx, bcc::robot_ops((int)robot)->prep(a, st));
     s = ensure_env_code(ctx, st);
     if (s != BCC_OK) return s;
     bcc::MlpState& m = ctx->mlp;
     BCC_CUDA(ctx, m.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)num_samples));
     BCC_CUDA(ctx, m.y.ensure((size_t)num_samples));
-    BCC_CUDA(ctx, bcc::launch_training_rows((int)robot, a, ctx->env_code.as<float>(), num_samples, seed,
+    BCC_CUDA(ctx, bcc::robot_ops((int)robot)->training_rows(a, ctx->env_code.as<float>(), num_samples, seed,
                                             m.x.as<uint16_t>(), m.y.as<uint8_t>(), st));
     BCC_CUDA(ctx, cudaStreamSynchronize(st));
     if (h_positive_fraction) {
@@ -712,14 +710,14 @@ bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, i
     bcc::PipelineArgs a;
     bcc_status s = prepare(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, nullptr, nullptr, st, a);
     if (s != BCC_OK) return s;
-    BCC_CUDA(ctx, bcc::launch_prep((int)robot, a, st));
+    BCC_CUDA(ctx, bcc::robot_ops((int)robot)->prep(a, st));
     s = ensure_env_code(ctx, st);
     if (s != BCC_OK) return s;
     bcc::MlpState& m = ctx->mlp;
     BCC_CUDA(ctx, m.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)num_samples));
     BCC_CUDA(ctx, m.y.ensure((size_t)num_samples));
     BCC_CUDA(ctx, m.logits.ensure(sizeof(float) * (size_t)num_samples));
-    BCC_CUDA(ctx, bcc::launch_training_rows((int)robot, a, ctx->env_code.as<float>(), num_samples, seed,
+    BCC_CUDA(ctx, bcc::robot_ops((int)robot)->training_rows(a, ctx->env_code.as<float>(), num_samples, seed,
                                             m.x.as<uint16_t>(), m.y.as<uint8_t>(), st));
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

@@ -11,6 +11,9 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace bcc {
@@ -36,7 +39,9 @@ constexpr int kPrimF4 = 5;          // float4 words per primitive record
 // capsule test (:114-127) for capsules (h = (0, 0, len/2) along the capsule
 // axis); all compare squared quantities with a strict < 0 like the reference.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool sphere_hits_prim(float4 s, const float4* __restrict__ rec) {
+// Squared distance from the sphere centre to the record's box core, and the
+// record's rounding radius.
+__device__ __forceinline__ float prim_core_d2(float4 s, const float4* __restrict__ rec, float* rho) {
     const float4 w0 = rec[0], w1 = rec[1], w2 = rec[2], w3 = rec[3];
     const float dx = s.x - w0.x, dy = s.y - w0.y, dz = s.z - w0.z;
     const float p1 = fmaf(w1.x, dx, fmaf(w1.y, dy, w1.z * dz));
@@ -45,8 +50,14 @@ __device__ __forceinline__ bool sphere_hits_prim(float4 s, const float4* __restr
     const float e1 = fmaxf(fabsf(p1) - w1.w, 0.0f);
     const float e2 = fmaxf(fabsf(p2) - w2.w, 0.0f);
     const float e3 = fmaxf(fabsf(p3) - w3.w, 0.0f);
-    const float sum = fmaf(e1, e1, fmaf(e2, e2, e3 * e3));
-    const float rr = s.w + w0.w;
+    *rho = w0.w;
+    return fmaf(e1, e1, fmaf(e2, e2, e3 * e3));
+}
+
+__device__ __forceinline__ bool sphere_hits_prim(float4 s, const float4* __restrict__ rec) {
+    float rho;
+    const float sum = prim_core_d2(s, rec, &rho);
+    const float rr = s.w + rho;
     return sum - rr * rr < 0.0f;
 }
 
@@ -91,71 +102,112 @@ __device__ __forceinline__ int reference_rank_to_sample(int r, int n) {
 }
 
 // ---------------------------------------------------------------------------
-// Table-driven forward kinematics in FP32.  frame k+1 = frame k * F_k * Rz(q_k)
-// with F_k from M::joint_tf; sphere centre = R_f * local + p_f.
+// Table-driven forward kinematics over a kinematic tree:
+//   frame k+1 = frame joint_parent[k] * F_k * J_k(q_k),
+// J = Rz(q) (revolute, type 0) or Tz(q) (prismatic, type 1), F_k from
+// M::joint_tf; sphere centre = R_f * local + p_f.  Scalar type T is float for
+// robots whose reference FK is float code (Panda) and double where the
+// reference evaluates its FK in double (Fetch, Baxter); centres are rounded to
+// float either way, as the reference does when it passes them to the tests.
+// Each sphere is emitted right after its frame is known, so a frame stays
+// live only while later joints or spheres still need it.
 // ---------------------------------------------------------------------------
-template <class M>
+template <class M, class T>
 struct Frames {
-    float R[M::dof + 1][9];
-    float p[M::dof + 1][3];
+    T R[M::dof + 1][9];
+    T p[M::dof + 1][3];
 };
 
+template <class M, int S, class T>
+__device__ __forceinline__ float4 fk_sphere(const Frames<M, T>& F) {
+    constexpr int f = M::sphere_frame[S];
+    constexpr T lx = (T)M::sphere_local[S][0];
+    constexpr T ly = (T)M::sphere_local[S][1];
+    constexpr T lz = (T)M::sphere_local[S][2];
+    float4 c;
+    c.x = (float)(F.R[f][0] * lx + F.R[f][1] * ly + F.R[f][2] * lz + F.p[f][0]);
+    c.y = (float)(F.R[f][3] * lx + F.R[f][4] * ly + F.R[f][5] * lz + F.p[f][1]);
+    c.z = (float)(F.R[f][6] * lx + F.R[f][7] * ly + F.R[f][8] * lz + F.p[f][2]);
+    c.w = M::sphere_radius[S];
+    return c;
+}
+
+// Write every sphere attached to frame FR into its sample-table position.
+template <class M, int FR, int S, class T>
+__device__ __forceinline__ void emit_one(const Frames<M, T>& F, float4* __restrict__ out) {
+    if constexpr (M::sphere_frame[S] == FR) {
+        constexpr int pos = M::table_pos[S];
+        out[pos] = fk_sphere<M, S, T>(F);
+    }
+}
+template <class M, int FR, class T, int... S>
+__device__ __forceinline__ void emit_frame(const Frames<M, T>& F, float4* __restrict__ out,
+                                           std::integer_sequence<int, S...>) {
+    (emit_one<M, FR, S, T>(F, out), ...);
+}
+
+__device__ __forceinline__ void sin_cos(float q, float* s, float* c) { sincosf(q, s, c); }
+__device__ __forceinline__ void sin_cos(double q, double* s, double* c) { sincos(q, s, c); }
+
 // One joint: compile-time constants of F_K are folded into the multiply-adds.
-template <class M, int K>
+template <class M, int K, class T>
 struct FkJoint {
-    __device__ __forceinline__ static void run(const float* q, Frames<M>& F) {
-        constexpr float f[12] = {
-            (float)M::joint_tf[K][0], (float)M::joint_tf[K][1], (float)M::joint_tf[K][2],
-            (float)M::joint_tf[K][3], (float)M::joint_tf[K][4], (float)M::joint_tf[K][5],
-            (float)M::joint_tf[K][6], (float)M::joint_tf[K][7], (float)M::joint_tf[K][8],
-            (float)M::joint_tf[K][9], (float)M::joint_tf[K][10], (float)M::joint_tf[K][11]};
-        float A[9];
+    __device__ __forceinline__ static void run(const float* q, Frames<M, T>& F, float4* __restrict__ out) {
+        constexpr int P = M::joint_parent[K];
+        static_assert(P <= K, "joints must follow their parents");
+        constexpr T f[12] = {
+            (T)M::joint_tf[K][0], (T)M::joint_tf[K][1], (T)M::joint_tf[K][2],
+            (T)M::joint_tf[K][3], (T)M::joint_tf[K][4], (T)M::joint_tf[K][5],
+            (T)M::joint_tf[K][6], (T)M::joint_tf[K][7], (T)M::joint_tf[K][8],
+            (T)M::joint_tf[K][9], (T)M::joint_tf[K][10], (T)M::joint_tf[K][11]};
+        T A[9];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
 #pragma unroll
             for (int b = 0; b < 3; ++b)
-                A[a * 3 + b] = F.R[K][a * 3 + 0] * f[0 * 4 + b] + F.R[K][a * 3 + 1] * f[1 * 4 + b] +
-                               F.R[K][a * 3 + 2] * f[2 * 4 + b];
-            F.p[K + 1][a] = F.R[K][a * 3 + 0] * f[3] + F.R[K][a * 3 + 1] * f[7] +
-                            F.R[K][a * 3 + 2] * f[11] + F.p[K][a];
+                A[a * 3 + b] = F.R[P][a * 3 + 0] * f[0 * 4 + b] + F.R[P][a * 3 + 1] * f[1 * 4 + b] +
+                               F.R[P][a * 3 + 2] * f[2 * 4 + b];
+            F.p[K + 1][a] = F.R[P][a * 3 + 0] * f[3] + F.R[P][a * 3 + 1] * f[7] +
+                            F.R[P][a * 3 + 2] * f[11] + F.p[P][a];
         }
-        float sq, cq;
-        sincosf(q[K], &sq, &cq);
+        const T qk = (T)q[K];
+        if constexpr (M::joint_type[K] == 0) {
+            T sq, cq;
+            sin_cos(qk, &sq, &cq);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            F.R[K + 1][a * 3 + 0] = A[a * 3 + 0] * cq + A[a * 3 + 1] * sq;
-            F.R[K + 1][a * 3 + 1] = A[a * 3 + 1] * cq - A[a * 3 + 0] * sq;
-            F.R[K + 1][a * 3 + 2] = A[a * 3 + 2];
+            for (int a = 0; a < 3; ++a) {
+                F.R[K + 1][a * 3 + 0] = A[a * 3 + 0] * cq + A[a * 3 + 1] * sq;
+                F.R[K + 1][a * 3 + 1] = A[a * 3 + 1] * cq - A[a * 3 + 0] * sq;
+                F.R[K + 1][a * 3 + 2] = A[a * 3 + 2];
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+#pragma unroll
+                for (int b = 0; b < 3; ++b) F.R[K + 1][a * 3 + b] = A[a * 3 + b];
+                F.p[K + 1][a] += A[a * 3 + 2] * qk;
+            }
         }
-        FkJoint<M, K + 1>::run(q, F);
+        emit_frame<M, K + 1, T>(F, out, std::make_integer_sequence<int, M::num_spheres>{});
+        FkJoint<M, K + 1, T>::run(q, F, out);
     }
 };
 
-template <class M>
-struct FkJoint<M, M::dof> {
-    __device__ __forceinline__ static void run(const float*, Frames<M>&) {}
+template <class M, class T>
+struct FkJoint<M, M::dof, T> {
+    __device__ __forceinline__ static void run(const float*, Frames<M, T>&, float4* __restrict__) {}
 };
 
+// All sphere centres of configuration q into out[table_pos[s]].
 template <class M>
-__device__ __forceinline__ void fk_frames(const float* q, Frames<M>& F) {
+__device__ __forceinline__ void fk_spheres(const float* q, float4* __restrict__ out) {
+    using T = typename std::conditional<M::fk_precision == 64, double, float>::type;
+    Frames<M, T> F;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) F.R[0][i] = (i % 4 == 0) ? 1.0f : 0.0f;
-    F.p[0][0] = F.p[0][1] = F.p[0][2] = 0.0f;
-    FkJoint<M, 0>::run(q, F);
-}
-
-template <class M, int S>
-__device__ __forceinline__ float4 fk_sphere(const Frames<M>& F) {
-    constexpr int f = M::sphere_frame[S];
-    constexpr float lx = (float)M::sphere_local[S][0];
-    constexpr float ly = (float)M::sphere_local[S][1];
-    constexpr float lz = (float)M::sphere_local[S][2];
-    float4 c;
-    c.x = F.R[f][0] * lx + F.R[f][1] * ly + F.R[f][2] * lz + F.p[f][0];
-    c.y = F.R[f][3] * lx + F.R[f][4] * ly + F.R[f][5] * lz + F.p[f][1];
-    c.z = F.R[f][6] * lx + F.R[f][7] * ly + F.R[f][8] * lz + F.p[f][2];
-    c.w = M::sphere_radius[S];
-    return c;
+    for (int i = 0; i < 9; ++i) F.R[0][i] = (i % 4 == 0) ? T(1) : T(0);
+    F.p[0][0] = F.p[0][1] = F.p[0][2] = T(0);
+    emit_frame<M, 0, T>(F, out, std::make_integer_sequence<int, M::num_spheres>{});
+    FkJoint<M, 0, T>::run(q, F, out);
 }
 
 // Bounded mbarrier wait: gives up after `limit` polls and reports false.

@@ -1,108 +1,32 @@
-// bcc_kernels.cu -- sm_100a kernels of the batch edge collision checker.
-//
-// Pipeline of one check (all on one stream):
-//   1. edge_steps_kernel   n per edge (reference discretisation, src/batch_cc.cu:103-107)
-//   2. scan_kernel         exclusive prefix sum of 32 n -> per-edge sample offsets
-//   3. fk_kernel           one thread per (edge, sample): FK of every robot sphere
-//                          into the sample table, env-independent, computed once
-//                          instead of once per environment as in the reference
-//   4. self_kernel         self-collision of every sample (src/utils.cuh:1192-5440),
-//                          OR-reduced per edge; env-independent
-//   5. swept_kernel        per (edge, link) AABB of the link's bounding sphere over
-//                          all the edge's samples (cull volume)
-//   6. check_kernel        CTA = one environment x a tile of edges.  The
-//                          environment's blob (primitive records + interval-mask
-//                          cull tables) is staged into shared memory once by a
-//                          cp.async.bulk copy and reused by every edge of the tile.
-//                          Each warp takes one edge at a time: lanes 0..9 turn the
-//                          link's swept AABB into three slab ranges and AND three
-//                          64-bit primitive masks (the cull), the surviving
-//                          (primitive, link) pairs are compacted, and the warp walks
-//                          (sample, pair) items 32 at a time in check order with a
-//                          warp-ballot exit on the first hit.
+// bcc_kernels.cu -- robot-independent kernels of the batch edge collision
+// checker (sm_100a): the sample-offset scan, the environment code of the
+// learned check order, shared-memory sizing, and the robot registry.  The
+// robot-templated pipeline lives in bcc_pipeline.cuh and is instantiated once
+// per robot in bcc_robot_<name>.cu.
 #include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include <cuda_bf16.h>
-
 #include "bcc_device.cuh"
 #include "bcc_kernels.h"
-#include "robot_panda.h"
+#include "bcc_mlp.h"
 
 namespace bcc {
 
-// ------------------------------------------------------------------ tables
-template <class M>
-struct DevTables {
-    int env_bound[M::num_env_groups];
-    int leaf_begin[M::num_env_groups + 1];
-    int leaves[M::num_env_leaves];
-    int self_bound[M::num_self_groups][2];
-    int self_pair_begin[M::num_self_groups + 1];
-    unsigned char self_pairs[M::num_self_pairs][2];
-    float sphere_radius[M::num_spheres];
-    float s_m[M::dof], s_a[M::dof];  // joint-limit scale q = u * s_m + s_a
-};
+extern const RobotOps kPandaOps;
+extern const RobotOps kFetchOps;
+extern const RobotOps kBaxterOps;
 
-__constant__ DevTables<PandaModel> c_tab_panda;
-
-template <class M>
-__device__ __forceinline__ const DevTables<M>& tab();
-template <>
-__device__ __forceinline__ const DevTables<PandaModel>& tab<PandaModel>() {
-    return c_tab_panda;
+const RobotOps* robot_ops(int robot) {
+    switch (robot) {
+        case 0: return &kPandaOps;
+        case 1: return &kFetchOps;
+        case 2: return &kBaxterOps;
+        default: return nullptr;
+    }
 }
 
-template <class M>
-static DevTables<M> host_tables() {
-    DevTables<M> t;
-    for (int g = 0; g < M::num_env_groups; ++g) t.env_bound[g] = M::env_bound[g];
-    for (int g = 0; g <= M::num_env_groups; ++g) t.leaf_begin[g] = M::env_leaf_begin[g];
-    for (int i = 0; i < M::num_env_leaves; ++i) t.leaves[i] = M::env_leaves[i];
-    // Self tables hold sample-table row positions, not sphere indices.
-    for (int g = 0; g < M::num_self_groups; ++g) {
-        t.self_bound[g][0] = M::table_pos[M::self_bound[g][0]];
-        t.self_bound[g][1] = M::table_pos[M::self_bound[g][1]];
-    }
-    for (int g = 0; g <= M::num_self_groups; ++g) t.self_pair_begin[g] = M::self_pair_begin[g];
-    for (int i = 0; i < M::num_self_pairs; ++i) {
-        t.self_pairs[i][0] = (unsigned char)M::table_pos[M::self_pairs[i][0]];
-        t.self_pairs[i][1] = (unsigned char)M::table_pos[M::self_pairs[i][1]];
-    }
-    for (int s = 0; s < M::num_spheres; ++s) t.sphere_radius[s] = M::sphere_radius[s];
-    for (int j = 0; j < M::dof; ++j) {
-        t.s_m[j] = M::s_m[j];
-        t.s_a[j] = M::s_a[j];
-    }
-    return t;
-}
-
-cudaError_t upload_robot_tables(int robot) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    DevTables<PandaModel> t = host_tables<PandaModel>();
-    return cudaMemcpyToSymbol(c_tab_panda, &t, sizeof(t));
-}
-
-// ------------------------------------------------------------------ 1. steps
-template <class M>
-__global__ void edge_steps_kernel(const float* __restrict__ edges, int E, int resolution,
-                                  int* __restrict__ steps) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E) return;
-    float s[M::dof], t[M::dof];
-#pragma unroll
-    for (int j = 0; j < M::dof; ++j) {
-        s[j] = edges[(size_t)e * 2 * M::dof + j];
-        t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
-    }
-    // Non-finite endpoints would give an unbounded step count: clamp, and let the
-    // host reject the resulting sample total (BCC_ERR_LIMIT).
-    const int n = edge_steps<M::dof>(s, t, resolution);
-    steps[e] = (n < 1 || n > (1 << 20)) ? (1 << 20) : n;
-}
-
-// ------------------------------------------------------------------ 2. scan
+// ------------------------------------------------------------------ scan
 // Single-CTA exclusive scan of 32*steps[e] into offs[e], offs[E] = total.
 // Sums run in 64 bits and every offset saturates at INT32_MAX, so a total too
 // large for the sample table can never wrap into a small, valid-looking one;
@@ -143,547 +67,29 @@ __global__ void scan_kernel(const int* __restrict__ steps, int E, int* __restric
     if (threadIdx.x == 0) offs[E] = (int)min(carry, 2147483647ll);
 }
 
-// ------------------------------------------------------------------ 3. FK
-template <class M, int S>
-struct WriteSpheres {
-    __device__ __forceinline__ static void run(const Frames<M>& F, float4* __restrict__ out) {
-        WriteSpheres<M, S - 1>::run(F, out);
-        constexpr int pos = M::table_pos[S - 1];
-        out[pos] = fk_sphere<M, S - 1>(F);
-    }
-};
-template <class M>
-struct WriteSpheres<M, 0> {
-    __device__ __forceinline__ static void run(const Frames<M>&, float4*) {}
-};
-
-// Sample table row: num_spheres float4 (centre xyz, radius) in table_pos order
-// (env-group bounds, then env leaves, then the rest), one row per (edge,
-// sample) in edge order then sample index order.
-template <class M>
-__global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges, int E,
-                                                 const int* __restrict__ steps,
-                                                 const int* __restrict__ offs,
-                                                 float4* __restrict__ table,
-                                                 int* __restrict__ row_edge) {
-    const int total = offs[E];
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= total) return;
-    // edge of this row: binary search over offs
-    int lo = 0, hi = E - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (offs[mid] <= row) lo = mid; else hi = mid - 1;
-    }
-    const int e = lo;
-    const int k = row - offs[e];
-    float s[M::dof], t[M::dof], q[M::dof];
-#pragma unroll
-    for (int j = 0; j < M::dof; ++j) {
-        s[j] = edges[(size_t)e * 2 * M::dof + j];
-        t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
-    }
-    edge_sample<M::dof>(s, t, steps[e], k, q);
-    Frames<M> F;
-    fk_frames<M>(q, F);
-    WriteSpheres<M, M::num_spheres>::run(F, table + (size_t)row * M::num_spheres);
-    row_edge[row] = e;
+cudaError_t launch_scan(const int* steps, int E, int* offs, cudaStream_t st) {
+    scan_kernel<<<1, 1024, 0, st>>>(steps, E, offs);
+    return cudaGetLastError();
 }
 
-// ------------------------------------------------------------------ 4. self
-__device__ __forceinline__ bool self_hit(float4 a, float4 b) {
-    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
-    const float rs = a.w + b.w;
-    return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) - rs * rs < 0.0f;
-}
-
-template <class M>
-__global__ void __launch_bounds__(128) self_kernel(const float4* __restrict__ table, int total,
-                                                   const int* __restrict__ row_edge,
-                                                   int* __restrict__ edge_self) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= total) return;
-    const float4* sp = table + (size_t)row * M::num_spheres;
-    const DevTables<M>& T = tab<M>();
-    bool hit = false;
-    for (int g = 0; g < M::num_self_groups && !hit; ++g) {
-        if (!self_hit(sp[T.self_bound[g][0]], sp[T.self_bound[g][1]])) continue;
-        for (int k = T.self_pair_begin[g]; k < T.self_pair_begin[g + 1]; ++k) {
-            if (self_hit(sp[T.self_pairs[k][0]], sp[T.self_pairs[k][1]])) {
-                hit = true;
-                break;
-            }
-        }
-    }
-    if (hit) atomicOr(edge_self + row_edge[row], 1);
-}
-
-// ------------------------------------------------------------------ 5. swept
-// One warp per edge: AABB (lo, hi) of every env group's bounding sphere over
-// the edge's samples, inflated by radius + 0.005 + cull margin.
-template <class M>
-__global__ void swept_kernel(const float4* __restrict__ table, const int* __restrict__ offs, int E,
-                             float4* __restrict__ swept) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= E) return;
-    const int r0 = offs[warp], r1 = offs[warp + 1];
-    const DevTables<M>& T = tab<M>();
-    for (int g = 0; g < M::num_env_groups; ++g) {
-        const int b = g;  // bounds lead every table row
-        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int r = r0 + lane; r < r1; r += 32) {
-            const float4 c = table[(size_t)r * M::num_spheres + b];
-            lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
-            hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
-        }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
-                hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
-            }
-        }
-        if (lane == 0) {
-            const float pad = T.sphere_radius[T.env_bound[g]] + kEnvInflate + kCullMargin;
-            const float4 l = make_float4(lo[0] - pad, lo[1] - pad, lo[2] - pad, 0.0f);
-            const float4 h = make_float4(hi[0] + pad, hi[1] + pad, hi[2] + pad, 0.0f);
-            swept[((size_t)warp * M::num_env_groups + g) * 2 + 0] = l;
-            swept[((size_t)warp * M::num_env_groups + g) * 2 + 1] = h;
-        }
-    }
-}
-
-// ------------------------------------------------------------------ 6. check
-// Slab index range of [lo, hi] on one axis of an environment's cull grid, as a
-// triangular table index; -1 when the interval misses every primitive.
-__device__ __forceinline__ int slab_tri(float lo, float hi, float g0, float inv) {
-    const float f0 = (lo - g0) * inv, f1 = (hi - g0) * inv;
-    if (!(f1 >= 0.0f) || !(f0 < (float)kGridSlabs)) return -1;
-    const int i0 = (int)fminf(fmaxf(floorf(f0), 0.0f), (float)(kGridSlabs - 1));
-    const int i1 = (int)fminf(fmaxf(floorf(f1), 0.0f), (float)(kGridSlabs - 1));
-    return tri_index(i0, i1);
-}
-
-// MODE 0: plain order, full walk.  MODE 1 (learned pipeline, phase 1): plain
-// order, first 32-item chunk only; a pair still undecided after it is queued
-// (with MLP rows for its segments) instead of getting a verdict.  MODE 2
-// (phase 3): the CTA's queued pairs, walked in descending segment score.
-//
-// check_tile processes the edges of one (environment, edge tile) work item
-// with the environment's blob already staged in shared memory; it is shared
-// by the one-CTA-per-item grid kernel and the persistent kernel.
-template <class M, int WARPS, int MODE>
-__device__ __forceinline__ void check_tile(const CheckParams& P, int env, int tile, int n_slots,
-                                           const unsigned char* smem, uint8_t (*s_perm)[kMaxSegments], float4 h0,
-                                           float4 h1) {
-    constexpr int G = M::num_env_groups;
-    const int e_begin = tile * P.edges_per_cta;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cta = tile * P.num_envs + env;
-    const uint32_t shape = __float_as_uint(h1.w);
-    const int np = (int)(shape & 0xffffu);
-    const int W = (int)(shape >> 16);  // 64-bit words per primitive mask
-    const float4* prim = reinterpret_cast<const float4*>(smem);
-    const uint64_t* masks = reinterpret_cast<const uint64_t*>(smem + (size_t)np * kPrimF4 * 16);
-    uint16_t* pairs = reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) +
-                      (size_t)warp * P.pairs_per_warp;
-    const DevTables<M>& T = tab<M>();
-
-    for (int slot = warp; slot < n_slots; slot += WARPS) {
-        const int e = MODE == 2 ? P.q_edges[(size_t)cta * P.edges_per_cta + slot] : e_begin + slot;
-        uint8_t* out = P.results + (size_t)e * P.num_envs + env;
-        const int self = P.edge_self[e];
-        if (np == 0 || self) {  // a self-colliding sample collides in every environment
-            if (lane == 0) *out = self ? 1 : 0;
-            continue;
-        }
-        // Cull: lane g < G intersects link g's swept box with the env's slab tables.
-        int tx = -1, ty = -1, tz = -1;
-        if (lane < G) {
-            const float4 lo = P.swept[((size_t)e * G + lane) * 2 + 0];
-            const float4 hi = P.swept[((size_t)e * G + lane) * 2 + 1];
-            tx = slab_tri(lo.x, hi.x, h0.x, h1.x);
-            ty = slab_tri(lo.y, hi.y, h0.y, h1.y);
-            tz = slab_tri(lo.z, hi.z, h0.z, h1.z);
-        }
-        const bool live = tx >= 0 && ty >= 0 && tz >= 0;
-        // Compact the surviving (primitive, link) pairs, link-major: for each link
-        // the whole warp writes that link's mask bits, lane l owning bits l, l + 32.
-        int C = 0;
-        const uint32_t lt = (1u << lane) - 1u;
-        for (int w = 0; w < W; ++w) {
-            uint64_t mine = 0;
-            if (live) {
-                mine = masks[((size_t)0 * kGridTri + tx) * W + w] & masks[((size_t)1 * kGridTri + ty) * W + w] &
-                       masks[((size_t)2 * kGridTri + tz) * W + w];
-            }
-#pragma unroll 1
-            for (int g = 0; g < G; ++g) {
-                const uint32_t mlo = __shfl_sync(0xffffffffu, (uint32_t)mine, g);
-                const uint32_t mhi = __shfl_sync(0xffffffffu, (uint32_t)(mine >> 32), g);
-                if ((mlo | mhi) == 0u) continue;
-                const int clo = __popc(mlo);
-                if ((mlo >> lane) & 1u) pairs[C + __popc(mlo & lt)] = (uint16_t)(((w * 64 + lane) << 4) | g);
-                if ((mhi >> lane) & 1u)
-                    pairs[C + clo + __popc(mhi & lt)] = (uint16_t)(((w * 64 + 32 + lane) << 4) | g);
-                C += clo + __popc(mhi);
-            }
-        }
-        __syncwarp();
-
-        // Walk (sample rank, pair) items, 32 per step, in check order.
-        bool collide = false, undecided = false;
-        unsigned long long n_chunks = 0, n_gates = 0, n_leaf = 0;
-        if (C > 0) {
-            const int n = P.steps[e];
-            const int total = kLanes * n * C;
-            const size_t row0 = (size_t)P.offs[e];
-            // Learned order: rank the edge's 4 n segments by their MLP score
-            // (descending, ties by index; NaN scores last).
-            const int nseg = 4 * n;
-            const int seg_row = MODE == 2 ? P.q_rows[(size_t)cta * P.edges_per_cta + slot] : -1;
-            const bool learned = MODE == 2 && seg_row >= 0 && nseg <= kMaxSegments;
-            if (learned) {
-                float v0 = lane < nseg ? P.logits[seg_row + lane] : -INFINITY;
-                float v1 = lane + 32 < nseg ? P.logits[seg_row + lane + 32] : -INFINITY;
-                v0 = isnan(v0) ? -INFINITY : v0;
-                v1 = isnan(v1) ? -INFINITY : v1;
-                int rank0 = 0, rank1 = 0;
-                for (int i = 0; i < nseg; ++i) {
-                    const float vi = __shfl_sync(0xffffffffu, i < 32 ? v0 : v1, i & 31);
-                    rank0 += (vi > v0 || (vi == v0 && i < lane)) ? 1 : 0;
-                    rank1 += (vi > v1 || (vi == v1 && i < lane + 32)) ? 1 : 0;
-                }
-                if (lane < nseg) s_perm[warp][rank0] = (uint8_t)lane;
-                if (lane + 32 < nseg) s_perm[warp][rank1] = (uint8_t)(lane + 32);
-                __syncwarp();
-            }
-            const int dr = 32 / C, dc = 32 % C;
-            int r = lane / C, c = lane - (lane / C) * C;
-            for (int w0 = 0; w0 < total; w0 += 32) {
-                bool gate = false;
-                int g = 0, p = 0, k = 0;
-                if (w0 + lane < total) {
-                    k = learned ? (int)s_perm[warp][r >> 3] * kSegment + (r & (kSegment - 1))
-                                : reference_rank_to_sample(r, n);
-                    const uint32_t pr = pairs[c];
-                    g = (int)(pr & 15u);
-                    p = (int)(pr >> 4);
-                    float4 bs = P.table[(row0 + (size_t)k) * M::num_spheres + g];
-                    bs.w += kEnvInflate;
-                    gate = sphere_hits_prim(bs, prim + p * kPrimF4);
-                }
-                ++n_chunks;
-                if (__any_sync(0xffffffffu, gate)) {
-                    ++n_gates;
-                    // Leaf work of every gated item, flattened over the warp: item j owns
-                    // leaf slots [incl_j - cnt_j, incl_j); each step tests 32 slots and the
-                    // warp stops at the first step with a hit.
-                    const int cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
-                    int incl = cnt;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += y;
-                    }
-                    const int L = __shfl_sync(0xffffffffu, incl, 31);
-                    const int first = T.leaf_begin[g];
-                    for (int t0 = 0; t0 < L; t0 += 32) {
-                        const int t = t0 + lane;
-                        // owner j: the first lane whose inclusive count exceeds t
-                        int j = 0;
-#pragma unroll
-                        for (int step = 16; step; step >>= 1) {
-                            const int v = __shfl_sync(0xffffffffu, incl, j + step - 1);
-                            if (v <= t) j += step;
-                        }
-                        const int j_incl = __shfl_sync(0xffffffffu, incl, j);
-                        const int j_cnt = __shfl_sync(0xffffffffu, cnt, j);
-                        const int j_first = __shfl_sync(0xffffffffu, first, j);
-                        const int j_k = __shfl_sync(0xffffffffu, k, j);
-                        const int j_p = __shfl_sync(0xffffffffu, p, j);
-                        bool hit = false;
-                        if (t < L) {
-                            const int leaf = j_first + (t - (j_incl - j_cnt));
-                            float4 ls = P.table[(row0 + (size_t)j_k) * M::num_spheres + G + leaf];
-                            ls.w += kEnvInflate;
-                            hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
-                        }
-                        ++n_leaf;
-                        if (__any_sync(0xffffffffu, hit)) {
-                            collide = true;
-                            break;
-                        }
-                    }
-                    if (collide) break;
-                }
-                // Probe: after the first chunk, queue the pair for the learned order
-                // only when much work remains; small remainders finish in plain order.
-                if (MODE == 1 && w0 == 0 && total - 32 >= P.queue_min_items) {
-                    undecided = true;
-                    break;
-                }
-                c += dc;
-                r += dr;
-                if (c >= C) {
-                    c -= C;
-                    ++r;
-                }
-            }
-        }
-        __syncwarp();
-        if (MODE == 1 && undecided) {
-            if (lane == 0) {
-                const int n = P.steps[e];
-                const int qi = atomicAdd(P.q_count + cta, 1);
-                int ro = -1;
-                if (4 * n <= kMaxSegments) {
-                    ro = atomicAdd(P.row_count, 4 * n);
-                    if (ro > P.row_cap - 4 * n) ro = -1;
-                }
-                P.q_edges[(size_t)cta * P.edges_per_cta + qi] = e;
-                P.q_rows[(size_t)cta * P.edges_per_cta + qi] = ro;
-            }
-            continue;
-        }
-        if (lane == 0) {
-            *out = collide ? 1 : 0;
-            if (P.counters) {
-                atomicAdd(P.counters + 0, 1ull);
-                atomicAdd(P.counters + 1, (unsigned long long)C);
-                atomicAdd(P.counters + 2, n_chunks);
-                atomicAdd(P.counters + 3, n_gates);
-                atomicAdd(P.counters + 4, n_leaf);
-                atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
-            }
-        }
-    }
-}
-
-__device__ __forceinline__ int tile_slots(const CheckParams& P, int env, int tile, int mode) {
-    if (mode == 2) return P.q_count[tile * P.num_envs + env];
-    const int e_begin = tile * P.edges_per_cta;
-    return min(P.edges_per_cta, P.num_edges - e_begin);
-}
-
-__device__ __forceinline__ uint32_t blob_bytes_of(float4 h1) {
-    const uint32_t shape = __float_as_uint(h1.w);
-    return (shape & 0xffffu) * kPrimF4 * 16u + 3u * kGridTri * (shape >> 16) * 8u;
-}
-
-// One CTA per (environment, edge tile): blockIdx.x = environment, blockIdx.y = tile.
-template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
-    const int env = blockIdx.x, tile = blockIdx.y;
-    const int n_slots = tile_slots(P, env, tile, MODE);
-    if (n_slots <= 0) return;
-    const float4 h0 = P.env_hdr[2 * env + 0];
-    const float4 h1 = P.env_hdr[2 * env + 1];
-    const uint32_t bytes = blob_bytes_of(h1);
-    if (bytes) {
-        if (threadIdx.x == 0) {
-            mbar_init(&bar, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)__float_as_uint(h0.w), bytes, &bar);
-        if (!mbar_wait_bounded(&bar, 0u, 1u << 22)) {
-            if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
-            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
-            return;
-        }
-    }
-    check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, s_perm, h0, h1);
-}
-
-// Persistent: a grid sized to the resident capacity pulls environment-major
-// work items (environment, edge tile) from an atomic counter, two at a time so
-// that consecutive items usually share the environment and its staged blob.
-constexpr int kItemsPerGrab = 2;
-
-template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32) check_persistent_kernel(CheckParams P) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
-    __shared__ int s_item;
-    const int tiles = (P.num_edges + P.edges_per_cta - 1) / P.edges_per_cta;
-    const long long items = (long long)P.num_envs * tiles;
-    if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    int staged = -1;
-    uint32_t phase = 0;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(P.work_counter, kItemsPerGrab);
-        __syncthreads();
-        const int first = s_item;
-        __syncthreads();
-        if (first >= items) break;
-        bool failed = false;
-        for (int item = first; item < first + kItemsPerGrab && item < items; ++item) {
-            const int env = item / tiles, tile = item - (item / tiles) * tiles;
-            const int n_slots = tile_slots(P, env, tile, MODE);
-            if (n_slots <= 0) continue;
-            const float4 h0 = P.env_hdr[2 * env + 0];
-            const float4 h1 = P.env_hdr[2 * env + 1];
-            if (env != staged) {
-                const uint32_t bytes = blob_bytes_of(h1);
-                __syncthreads();  // every warp is done with the previous blob
-                if (bytes) {
-                    if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)__float_as_uint(h0.w), bytes, &bar);
-                    const bool ok = mbar_wait_bounded(&bar, phase, 1u << 22);
-                    if (__syncthreads_or(!ok)) {
-                        if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
-                        mbar_wait_bounded(&bar, phase, 1u << 22);
-                        failed = true;
-                        break;
-                    }
-                    phase ^= 1u;
-                }
-                staged = env;
-            }
-            check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, s_perm, h0, h1);
-        }
-        if (failed) break;
-        __syncthreads();
-    }
-}
-
-// ------------------------------------------------------------------ launchers
-size_t check_smem_bytes(int max_prims, size_t blob_smem, int warps) {
-    const size_t ppw = (size_t)((max_prims * 16 + 7) & ~7);
+// ------------------------------------------------------------------ sizing
+// Dynamic shared memory of a check CTA: the largest environment blob plus,
+// per warp, a (primitive, link) pair list of max_prims x groups entries.
+size_t check_smem_bytes(int max_prims, int groups, size_t blob_smem, int warps) {
+    const size_t ppw = (size_t)((max_prims * groups + 7) & ~7);
     return blob_smem + (size_t)warps * ppw * sizeof(uint16_t);
 }
 
-template <class M>
-static cudaError_t run_steps(const PipelineArgs& a, cudaStream_t st) {
-    const int E = a.num_edges;
-    if (a.stage_events) cudaEventRecord(a.stage_events[0], st);
-    edge_steps_kernel<M><<<(E + 255) / 256, 256, 0, st>>>(a.d_edges, E, a.resolution, a.steps);
-    scan_kernel<<<1, 1024, 0, st>>>(a.steps, E, a.offs);
-    return cudaGetLastError();
+size_t records_smem_bytes(int max_prims, int groups, int warps) {
+    const size_t ppw = (size_t)((max_prims * groups + 7) & ~7);
+    return (size_t)max_prims * kPrimF4 * 16 + (size_t)warps * ppw * sizeof(uint16_t);
 }
 
-template <class M, int W, int MODE>
-static cudaError_t launch_check_wm(CheckParams P, int E, cudaStream_t st) {
-    P.pairs_per_warp = (P.max_prims * M::num_env_groups + 7) & ~7;
-    const size_t smem = P.blob_smem + (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
-    if (P.persistent) {
-        cudaError_t err = cudaFuncSetAttribute(check_persistent_kernel<M, W, MODE>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (err != cudaSuccess) return err;
-        int per_sm = 0, dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, check_persistent_kernel<M, W, MODE>, W * 32, smem);
-        if (err != cudaSuccess) return err;
-        const long long items = (long long)P.num_envs * ((E + P.edges_per_cta - 1) / P.edges_per_cta);
-        long long grid = (long long)std::max(per_sm, 1) * std::max(sms, 1);
-        grid = std::min(grid, (items + kItemsPerGrab - 1) / kItemsPerGrab);
-        err = cudaMemsetAsync(P.work_counter, 0, sizeof(int), st);
-        if (err != cudaSuccess) return err;
-        check_persistent_kernel<M, W, MODE><<<(unsigned)std::max(grid, 1ll), W * 32, smem, st>>>(P);
-        return cudaGetLastError();
-    }
-    cudaError_t err = cudaFuncSetAttribute(check_kernel<M, W, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
-    if (err != cudaSuccess) return err;
-    dim3 grid(P.num_envs, (E + P.edges_per_cta - 1) / P.edges_per_cta);
-    check_kernel<M, W, MODE><<<grid, W * 32, smem, st>>>(P);
-    return cudaGetLastError();
+int check_grid_size(const PipelineArgs& a) {
+    return a.num_envs * ((a.num_edges + a.edges_per_cta - 1) / a.edges_per_cta);
 }
 
-template <class M, int W>
-static cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st, int mode) {
-    switch (mode) {
-        case 1: return launch_check_wm<M, W, 1>(P, E, st);
-        case 2: return launch_check_wm<M, W, 2>(P, E, st);
-        default: return launch_check_wm<M, W, 0>(P, E, st);
-    }
-}
-
-template <class M>
-static cudaError_t run_check(const PipelineArgs& a, cudaStream_t st) {
-    const int E = a.num_edges;
-    const int R = a.total_rows;
-    cudaEvent_t* ev = a.stage_events;
-    if (ev) cudaEventRecord(ev[1], st);
-    if (R > 0) {
-        fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
-    }
-    if (ev) cudaEventRecord(ev[2], st);
-    cudaError_t err = cudaMemsetAsync(a.edge_self, 0, sizeof(int) * E, st);
-    if (err != cudaSuccess) return err;
-    if (R > 0) self_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
-    if (ev) cudaEventRecord(ev[3], st);
-    swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept);
-    if (ev) cudaEventRecord(ev[4], st);
-
-    CheckParams P;
-    P.blobs = a.blobs;
-    P.env_hdr = a.env_hdr;
-    P.num_envs = a.num_envs;
-    P.num_edges = E;
-    P.max_prims = a.max_prims;
-    P.blob_smem = a.blob_smem;
-    P.edges_per_cta = a.edges_per_cta;
-    P.steps = a.steps;
-    P.offs = a.offs;
-    P.table = a.table;
-    P.swept = a.swept;
-    P.edge_self = a.edge_self;
-    P.results = a.d_results;
-    P.error_flag = a.error_flag;
-    P.counters = a.counters;
-    P.q_count = a.q_count;
-    P.q_edges = a.q_edges;
-    P.q_rows = a.q_rows;
-    P.row_count = a.row_count;
-    P.row_cap = a.row_cap;
-    P.logits = a.logits;
-    P.queue_min_items = a.queue_min_items;
-    P.persistent = a.persistent;
-    P.work_counter = a.work_counter;
-    switch (a.warps) {
-        case 8: err = launch_check_w<M, 8>(P, E, st, a.mode); break;
-        case 4: err = launch_check_w<M, 4>(P, E, st, a.mode); break;
-        case 2: err = launch_check_w<M, 2>(P, E, st, a.mode); break;
-        case 1: err = launch_check_w<M, 1>(P, E, st, a.mode); break;
-        default: return cudaErrorInvalidValue;
-    }
-    if (ev) cudaEventRecord(ev[5], st);
-    return err;
-}
-
-cudaError_t launch_steps(int robot, const PipelineArgs& a, cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    return run_steps<PandaModel>(a, st);
-}
-
-cudaError_t launch_check(int robot, const PipelineArgs& a, cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    return run_check<PandaModel>(a, st);
-}
-
-int robot_num_spheres(int robot) { return robot == 0 ? PandaModel::num_spheres : -1; }
-int robot_num_env_groups(int robot) { return robot == 0 ? PandaModel::num_env_groups : -1; }
-int robot_dof(int robot) { return robot == 0 ? PandaModel::dof : -1; }
-
-}  // namespace bcc
-
-// ======================================================================
-// Learned check order: environment code, MLP features, training rows.
-// ======================================================================
-namespace bcc {
-
+// ------------------------------------------------------------------ environment code
 // 32-value environment code (one warp per environment): [0..3] counts of
 // sphere-like, capsule-like and box-like primitives and the total, / 64;
 // [4..27] for 8 fixed anchor points the distance from the anchor to the
@@ -737,7 +143,7 @@ __global__ void env_encode_kernel(const float4* __restrict__ blobs, const float4
             for (int k = 0; k < 3; ++k) best[a][k] = fminf(best[a][k], __shfl_xor_sync(0xffffffffu, best[a][k], o));
     }
     if (lane == 0) {
-        float* c = code + (size_t)env * 32;
+        float* c = code + (size_t)env * kEnvCode;
         c[0] = cnt[0] / 64.0f;
         c[1] = cnt[1] / 64.0f;
         c[2] = cnt[2] / 64.0f;
@@ -749,361 +155,9 @@ __global__ void env_encode_kernel(const float4* __restrict__ blobs, const float4
     }
 }
 
-// One MLP feature row: joints normalised to [-1, 1] by the joint limits, the
-// environment code, zeros; BF16, 48 values (96 bytes).
-template <class M>
-__device__ __forceinline__ void write_features(const float* q, const float* code, uint16_t* dst) {
-    const DevTables<M>& T = tab<M>();
-    float f[48];
-#pragma unroll
-    for (int j = 0; j < 48; ++j) f[j] = 0.0f;
-#pragma unroll
-    for (int j = 0; j < M::dof; ++j) f[j] = 2.0f * (q[j] - T.s_a[j]) / T.s_m[j] - 1.0f;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) f[7 + j] = code[j];
-    uint32_t w[24];
-#pragma unroll
-    for (int j = 0; j < 24; ++j) {
-        __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
-        w[j] = *reinterpret_cast<uint32_t*>(&h);
-    }
-    uint4* d = reinterpret_cast<uint4*>(dst);
-#pragma unroll
-    for (int j = 0; j < 6; ++j) d[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
-}
-
-// Features of every queued pair's segments: row ro + j is segment j scored at
-// its middle sample k = 8 j + 4.  One warp per queued pair.
-template <class M>
-__global__ void queue_features_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
-                                      uint16_t* __restrict__ x) {
-    const int cta = blockIdx.x;
-    const int env = cta % P.num_envs;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nq = P.q_count[cta];
-    for (int slot = warp; slot < nq; slot += blockDim.x >> 5) {
-        const int ro = P.q_rows[(size_t)cta * P.edges_per_cta + slot];
-        if (ro < 0) continue;
-        const int e = P.q_edges[(size_t)cta * P.edges_per_cta + slot];
-        const int n = P.steps[e];
-        float s[M::dof], t[M::dof], q[M::dof];
-#pragma unroll
-        for (int j = 0; j < M::dof; ++j) {
-            s[j] = edges[(size_t)e * 2 * M::dof + j];
-            t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
-        }
-        for (int seg = lane; seg < 4 * n; seg += 32) {
-            edge_sample<M::dof>(s, t, n, seg * kSegment + kSegment / 2, q);
-            write_features<M>(q, code + (size_t)env * 32, x + (size_t)(ro + seg) * 48);
-        }
-    }
-}
-
-// Training rows: row i draws (environment, edge, sample) from a hash of
-// (seed, i); features as above at that sample; label = the sample's
-// environment collision (gate then leaves, every primitive).
-__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
-    z += 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-
-template <class M>
-__global__ void training_rows_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
-                                     long long rows, unsigned long long seed, uint16_t* __restrict__ x,
-                                     uint8_t* __restrict__ y) {
-    constexpr int G = M::num_env_groups;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= rows) return;
-    const unsigned long long h1 = mix64(seed ^ (unsigned long long)i), h2 = mix64(h1), h3 = mix64(h2);
-    const int env = (int)(h1 % (unsigned long long)P.num_envs);
-    const int e = (int)(h2 % (unsigned long long)P.num_edges);
-    const int n = P.steps[e];
-    const int k = (int)(h3 % (unsigned long long)(kLanes * n));
-    float s[M::dof], t[M::dof], q[M::dof];
-#pragma unroll
-    for (int j = 0; j < M::dof; ++j) {
-        s[j] = edges[(size_t)e * 2 * M::dof + j];
-        t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
-    }
-    edge_sample<M::dof>(s, t, n, k, q);
-    write_features<M>(q, code + (size_t)env * 32, x + (size_t)i * 48);
-    const float4 hd0 = P.env_hdr[2 * env], hd1 = P.env_hdr[2 * env + 1];
-    const float4* rec = P.blobs + __float_as_uint(hd0.w);
-    const int np = (int)(__float_as_uint(hd1.w) & 0xffffu);
-    const float4* row = P.table + ((size_t)P.offs[e] + k) * M::num_spheres;
-    const DevTables<M>& T = tab<M>();
-    bool hit = false;
-    for (int p = 0; p < np && !hit; ++p) {
-        const float4* r = rec + p * kPrimF4;
-        for (int g = 0; g < G && !hit; ++g) {
-            float4 b = row[g];
-            b.w += kEnvInflate;
-            if (!sphere_hits_prim(b, r)) continue;
-            for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1] && !hit; ++li) {
-                float4 l = row[G + li];
-                l.w += kEnvInflate;
-                hit = sphere_hits_prim(l, r);
-            }
-        }
-    }
-    y[i] = hit ? 1 : 0;
-}
-
-int check_grid_size(const PipelineArgs& a) {
-    return a.num_envs * ((a.num_edges + a.edges_per_cta - 1) / a.edges_per_cta);
-}
-
-static CheckParams params_of(const PipelineArgs& a) {
-    CheckParams P{};
-    P.blobs = a.blobs;
-    P.env_hdr = a.env_hdr;
-    P.num_envs = a.num_envs;
-    P.num_edges = a.num_edges;
-    P.max_prims = a.max_prims;
-    P.blob_smem = a.blob_smem;
-    P.edges_per_cta = a.edges_per_cta;
-    P.steps = a.steps;
-    P.offs = a.offs;
-    P.table = a.table;
-    P.swept = a.swept;
-    P.edge_self = a.edge_self;
-    P.results = a.d_results;
-    P.error_flag = a.error_flag;
-    P.q_count = a.q_count;
-    P.q_edges = a.q_edges;
-    P.q_rows = a.q_rows;
-    P.row_count = a.row_count;
-    P.row_cap = a.row_cap;
-    P.logits = a.logits;
-    P.counters = a.counters;
-    P.queue_min_items = a.queue_min_items;
-    P.persistent = a.persistent;
-    P.work_counter = a.work_counter;
-    return P;
-}
-
-// Environment check only (the FK/self/swept stages already ran), in a.mode.
-cudaError_t launch_check_mode(int robot, const PipelineArgs& a, cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    using M = PandaModel;
-    CheckParams P = params_of(a);
-    switch (a.warps) {
-        case 8: return launch_check_w<M, 8>(P, a.num_edges, st, a.mode);
-        case 4: return launch_check_w<M, 4>(P, a.num_edges, st, a.mode);
-        case 2: return launch_check_w<M, 2>(P, a.num_edges, st, a.mode);
-        case 1: return launch_check_w<M, 1>(P, a.num_edges, st, a.mode);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
 cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st) {
     if (num_envs <= 0) return cudaSuccess;
     env_encode_kernel<<<(num_envs * 32 + 255) / 256, 256, 0, st>>>(blobs, env_hdr, num_envs, code);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_queue_features(int robot, const PipelineArgs& a, const float* env_code, uint16_t* x, int grid,
-                                  cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    if (grid <= 0) return cudaSuccess;
-    queue_features_kernel<PandaModel><<<grid, 128, 0, st>>>(params_of(a), a.d_edges, env_code, x);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_training_rows(int robot, const PipelineArgs& a, const float* env_code, long long rows,
-                                 unsigned long long seed, uint16_t* x, uint8_t* y, cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    if (rows <= 0) return cudaSuccess;
-    training_rows_kernel<PandaModel><<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(params_of(a), a.d_edges, env_code,
-                                                                                  rows, seed, x, y);
-    return cudaGetLastError();
-}
-
-}  // namespace bcc
-
-// ======================================================================
-// Records variant of the environment check (used by the allocation-free entry
-// point): works from the host-packed rounded-box records of bcc_pack_envs
-// (no interval-mask tables) and culls (primitive, link) pairs with an exact
-// AABB overlap test, one primitive per lane.  The walk over (sample, pair)
-// items is the same as check_kernel's.
-// ======================================================================
-namespace bcc {
-
-template <class M, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) check_records_kernel(RecordsParams P) {
-    constexpr int G = M::num_env_groups;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    __shared__ float4 boxes[WARPS][G][2];
-
-    const int env = blockIdx.x;
-    const int e_begin = blockIdx.y * P.edges_per_cta;
-    const int e_end = min(e_begin + P.edges_per_cta, P.num_edges);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p_begin = P.env_off[env];
-    const int np = P.env_off[env + 1] - p_begin;
-
-    const float4* prim = reinterpret_cast<const float4*>(smem);
-    uint16_t* pairs = reinterpret_cast<uint16_t*>(smem + (size_t)P.max_prims * kPrimF4 * 16) +
-                      (size_t)warp * P.pairs_per_warp;
-    if (np < 0 || np > P.max_prims) {  // shared memory was sized from the caller's max_prims
-        if (threadIdx.x == 0) atomicOr(P.error_flag, 2);
-        return;
-    }
-    if (np > 0) {
-        if (threadIdx.x == 0) {
-            mbar_init(&bar, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (threadIdx.x == 0)
-            bulk_copy_g2s(smem, P.records + (size_t)p_begin * kPrimF4, (uint32_t)np * kPrimF4 * 16u, &bar);
-        if (!mbar_wait_bounded(&bar, 0u, 1u << 22)) {
-            if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
-            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
-            return;
-        }
-    }
-    const DevTables<M>& T = tab<M>();
-    const uint32_t lt = (1u << lane) - 1u;
-
-    for (int e = e_begin + warp; e < e_end; e += WARPS) {
-        uint8_t* out = P.results + (size_t)e * P.num_envs + env;
-        const int self = P.edge_self[e];
-        if (np == 0 || self) {
-            if (lane == 0) *out = self ? 1 : 0;
-            continue;
-        }
-        if (lane < G) {
-            boxes[warp][lane][0] = P.swept[((size_t)e * G + lane) * 2 + 0];
-            boxes[warp][lane][1] = P.swept[((size_t)e * G + lane) * 2 + 1];
-        }
-        __syncwarp();
-        // Exact AABB cull, one primitive per lane; pairs compacted link-major
-        // within each block of 32 primitives.
-        int C = 0;
-        for (int p0 = 0; p0 < np; p0 += 32) {
-            const int p = p0 + lane;
-            uint32_t mask = 0;
-            if (p < np) {
-                const float4 c = prim[p * kPrimF4 + 0];
-                const float4 h = prim[p * kPrimF4 + 4];
-#pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    const float4 lo = boxes[warp][g][0], hi = boxes[warp][g][1];
-                    const bool ov = c.x - h.x <= hi.x && c.x + h.x >= lo.x && c.y - h.y <= hi.y &&
-                                    c.y + h.y >= lo.y && c.z - h.z <= hi.z && c.z + h.z >= lo.z;
-                    mask |= (uint32_t)ov << g;
-                }
-            }
-#pragma unroll 1
-            for (int g = 0; g < G; ++g) {
-                const uint32_t bits = __ballot_sync(0xffffffffu, (mask >> g) & 1u);
-                if ((mask >> g) & 1u) pairs[C + __popc(bits & lt)] = (uint16_t)((p << 4) | g);
-                C += __popc(bits);
-            }
-        }
-        __syncwarp();
-
-        bool collide = false;
-        if (C > 0) {
-            const int n = P.steps[e];
-            const int total = kLanes * n * C;
-            const size_t row0 = (size_t)P.offs[e];
-            const int dr = 32 / C, dc = 32 % C;
-            int r = lane / C, c = lane - (lane / C) * C;
-            for (int w0 = 0; w0 < total; w0 += 32) {
-                bool gate = false;
-                int g = 0, p = 0, k = 0;
-                if (w0 + lane < total) {
-                    k = reference_rank_to_sample(r, n);
-                    const uint32_t pr = pairs[c];
-                    g = (int)(pr & 15u);
-                    p = (int)(pr >> 4);
-                    float4 bs = P.table[(row0 + (size_t)k) * M::num_spheres + g];
-                    bs.w += kEnvInflate;
-                    gate = sphere_hits_prim(bs, prim + p * kPrimF4);
-                }
-                if (__any_sync(0xffffffffu, gate)) {
-                    const int cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
-                    int incl = cnt;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += y;
-                    }
-                    const int L = __shfl_sync(0xffffffffu, incl, 31);
-                    const int first = T.leaf_begin[g];
-                    for (int t0 = 0; t0 < L; t0 += 32) {
-                        const int t = t0 + lane;
-                        int j = 0;
-#pragma unroll
-                        for (int step = 16; step; step >>= 1) {
-                            const int v = __shfl_sync(0xffffffffu, incl, j + step - 1);
-                            if (v <= t) j += step;
-                        }
-                        const int j_incl = __shfl_sync(0xffffffffu, incl, j);
-                        const int j_cnt = __shfl_sync(0xffffffffu, cnt, j);
-                        const int j_first = __shfl_sync(0xffffffffu, first, j);
-                        const int j_k = __shfl_sync(0xffffffffu, k, j);
-                        const int j_p = __shfl_sync(0xffffffffu, p, j);
-                        bool hit = false;
-                        if (t < L) {
-                            const int leaf = j_first + (t - (j_incl - j_cnt));
-                            float4 ls = P.table[(row0 + (size_t)j_k) * M::num_spheres + G + leaf];
-                            ls.w += kEnvInflate;
-                            hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
-                        }
-                        if (__any_sync(0xffffffffu, hit)) {
-                            collide = true;
-                            break;
-                        }
-                    }
-                    if (collide) break;
-                }
-                c += dc;
-                r += dr;
-                if (c >= C) {
-                    c -= C;
-                    ++r;
-                }
-            }
-        }
-        __syncwarp();
-        if (lane == 0) *out = collide ? 1 : 0;
-    }
-}
-
-size_t records_smem_bytes(int max_prims, int warps) {
-    const size_t ppw = (size_t)((max_prims * 16 + 7) & ~7);
-    return (size_t)max_prims * kPrimF4 * 16 + (size_t)warps * ppw * sizeof(uint16_t);
-}
-
-cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    using M = PandaModel;
-    const int E = a.num_edges;
-    const int R = a.total_rows;
-    if (R > 0) fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
-    if (R > 0) self_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
-    swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_check_records(int robot, RecordsParams P, cudaStream_t st) {
-    if (robot != 0) return cudaErrorInvalidValue;
-    using M = PandaModel;
-    constexpr int W = 4;
-    P.pairs_per_warp = (P.max_prims * 16 + 7) & ~7;
-    const size_t smem = records_smem_bytes(P.max_prims, W);
-    cudaError_t err = cudaFuncSetAttribute(check_records_kernel<M, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem);
-    if (err != cudaSuccess) return err;
-    dim3 grid(P.num_envs, (P.num_edges + P.edges_per_cta - 1) / P.edges_per_cta);
-    check_records_kernel<M, W><<<grid, W * 32, smem, st>>>(P);
     return cudaGetLastError();
 }
 

@@ -91,16 +91,6 @@ struct PipelineArgs {
     int* work_counter;
 };
 
-cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st);
-// Learned-order helpers (bcc_kernels.cu).
-cudaError_t launch_check_mode(int robot, const PipelineArgs& a, cudaStream_t st);
-cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st);
-cudaError_t launch_queue_features(int robot, const PipelineArgs& a, const float* env_code, uint16_t* x, int grid,
-                                  cudaStream_t st);
-cudaError_t launch_training_rows(int robot, const PipelineArgs& a, const float* env_code, long long rows,
-                                 unsigned long long seed, uint16_t* x, uint8_t* y, cudaStream_t st);
-int check_grid_size(const PipelineArgs& a);
-
 // Environment check from host-packed records (bcc_pack_envs format), exact
 // AABB cull; used by the allocation-free entry point.
 struct RecordsParams {
@@ -120,18 +110,74 @@ struct RecordsParams {
     int* error_flag;
 };
 
-cudaError_t upload_robot_tables(int robot);
-// FK table, self-collision and swept volumes only (no environment check).
-cudaError_t launch_prep(int robot, const PipelineArgs& a, cudaStream_t st);
-cudaError_t launch_check_records(int robot, RecordsParams P, cudaStream_t st);
-size_t records_smem_bytes(int max_prims, int warps);
-// Stage 1: steps + sample offsets (total rows land in offs[E]).
-cudaError_t launch_steps(int robot, const PipelineArgs& a, cudaStream_t st);
-// Stage 2: FK table, self-collision, swept volumes, environment check.
-cudaError_t launch_check(int robot, const PipelineArgs& a, cudaStream_t st);
-size_t check_smem_bytes(int max_prims, size_t blob_smem, int warps);
-int robot_num_spheres(int robot);
-int robot_num_env_groups(int robot);
-int robot_dof(int robot);
+// Limits every robot model must respect (checked at compile time by the
+// robot's translation unit): link groups (one cull lane each) and sample-table
+// row width.
+constexpr int kMaxEnvGroups = 32;
+constexpr int kMaxTableSpheres = 128;
+constexpr int kRecordsWarps = 4;  // warps per CTA of the records check kernel
+
+// One robot's pipeline, instantiated in its own translation unit
+// (bcc_robot_<name>.cu) from the templates of bcc_pipeline.cuh.
+struct RobotOps {
+    int robot;               // bcc_robot id
+    int dof;
+    int num_spheres;         // sample-table row width (float4 per sample)
+    int num_env_groups;
+    int max_prims;           // primitives per environment the pair packing allows
+    cudaError_t (*upload_tables)();  // robot tables -> __constant__ of the current device
+    // Stage 1: steps + sample offsets (total rows land in offs[E]).
+    cudaError_t (*steps)(const PipelineArgs& a, cudaStream_t st);
+    // Stage 2: FK table, self-collision, swept volumes, environment check.
+    cudaError_t (*check)(const PipelineArgs& a, cudaStream_t st);
+    // FK table, self-collision and swept volumes only.
+    cudaError_t (*prep)(const PipelineArgs& a, cudaStream_t st);
+    // Environment check only, in a.mode.
+    cudaError_t (*check_mode)(const PipelineArgs& a, cudaStream_t st);
+    cudaError_t (*queue_features)(const PipelineArgs& a, const float* env_code, uint16_t* x, int grid,
+                                  cudaStream_t st);
+    cudaError_t (*training_rows)(const PipelineArgs& a, const float* env_code, long long rows,
+                                 unsigned long long seed, uint16_t* x, uint8_t* y, cudaStream_t st);
+    cudaError_t (*check_records)(RecordsParams P, cudaStream_t st);
+};
+
+// null for a robot this library was not built with.
+const RobotOps* robot_ops(int robot);
+
+// Robot-independent kernels (bcc_kernels.cu).
+cudaError_t launch_scan(const int* steps, int E, int* offs, cudaStream_t st);
+cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st);
+int check_grid_size(const PipelineArgs& a);
+size_t check_smem_bytes(int max_prims, int groups, size_t blob_smem, int warps);
+size_t records_smem_bytes(int max_prims, int groups, int warps);
+
+inline CheckParams params_of(const PipelineArgs& a) {
+    CheckParams P{};
+    P.blobs = a.blobs;
+    P.env_hdr = a.env_hdr;
+    P.num_envs = a.num_envs;
+    P.num_edges = a.num_edges;
+    P.max_prims = a.max_prims;
+    P.blob_smem = a.blob_smem;
+    P.edges_per_cta = a.edges_per_cta;
+    P.steps = a.steps;
+    P.offs = a.offs;
+    P.table = a.table;
+    P.swept = a.swept;
+    P.edge_self = a.edge_self;
+    P.results = a.d_results;
+    P.error_flag = a.error_flag;
+    P.counters = a.counters;
+    P.q_count = a.q_count;
+    P.q_edges = a.q_edges;
+    P.q_rows = a.q_rows;
+    P.row_count = a.row_count;
+    P.row_cap = a.row_cap;
+    P.logits = a.logits;
+    P.queue_min_items = a.queue_min_items;
+    P.persistent = a.persistent;
+    P.work_counter = a.work_counter;
+    return P;
+}
 
 }  // namespace bcc

@@ -10,7 +10,7 @@
 // buffers live in the fixed file-scope arrays below.
 //
 // Limits: at most kMaxEdges edges and kMaxRows discretised samples (the sum of
-// 32 n over the edges) per call; about 5 MB of device memory per GPU that loads
+// 32 n over the edges) per call; about 9 MB of device memory per GPU that loads
 // the library, held until the process exits.
 //
 // All calls share these arrays, and each call leaves its contents behind;
@@ -26,14 +26,13 @@
 #include "../../include/bcc.h"
 #include "bcc_device.cuh"
 #include "bcc_kernels.h"
-#include "robot_panda.h"
 
 namespace {
 
 constexpr int kMaxEdges = 1024;
 constexpr int kMaxRows = 4096;
-constexpr int kNumSpheresMax = bcc::PandaModel::num_spheres;
-constexpr int kGroupsMax = bcc::PandaModel::num_env_groups;
+constexpr int kNumSpheresMax = bcc::kMaxTableSpheres;  // widest sample-table row of any robot
+constexpr int kGroupsMax = bcc::kMaxEnvGroups;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) int g_steps[kMaxEdges];
@@ -53,14 +52,15 @@ struct Scratch {
     int* row_edge = nullptr;
     int* error = nullptr;
     bool ready = false;
+    bool tables[3] = {false, false, false};  // robot tables uploaded to this device
 };
 
 Scratch g_scratch[kMaxDevices];
 std::mutex g_setup_mutex;
 
 // Device addresses of the file-scope arrays (the host-side names are only
-// stand-ins) and the robot tables, once per device with that device current.
-cudaError_t setup_device(int dev, Scratch*& out) {
+// stand-ins) and the robot's tables, once per device with that device current.
+cudaError_t setup_device(int dev, const bcc::RobotOps* ops, Scratch*& out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     Scratch& s = g_scratch[dev];
     if (!s.ready) {
@@ -72,8 +72,12 @@ cudaError_t setup_device(int dev, Scratch*& out) {
         if ((e = cudaGetSymbolAddress((void**)&s.table, g_table)) != cudaSuccess) return e;
         if ((e = cudaGetSymbolAddress((void**)&s.row_edge, g_row_edge)) != cudaSuccess) return e;
         if ((e = cudaGetSymbolAddress((void**)&s.error, g_error)) != cudaSuccess) return e;
-        if ((e = bcc::upload_robot_tables(BCC_ROBOT_PANDA)) != cudaSuccess) return e;
         s.ready = true;
+    }
+    if (!s.tables[ops->robot]) {
+        cudaError_t e = ops->upload_tables();
+        if (e != cudaSuccess) return e;
+        s.tables[ops->robot] = true;
     }
     out = &s;
     return cudaSuccess;
@@ -84,17 +88,21 @@ cudaError_t setup_device(int dev, Scratch*& out) {
 extern "C" bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records, const int32_t* d_env_offsets,
                                         int32_t num_envs, int32_t max_prims_per_env, const float* d_edges,
                                         int32_t num_edges, int32_t resolution, uint8_t* d_results, void* stream) {
-    if (robot != BCC_ROBOT_PANDA) return BCC_ERR_NOT_SUPPORTED;
+    const bcc::RobotOps* ops = bcc::robot_ops((int)robot);
+    if (!ops) return BCC_ERR_NOT_SUPPORTED;
     if (num_envs < 0 || num_edges < 0 || resolution <= 0 || max_prims_per_env < 0) return BCC_ERR_INVALID_ARGUMENT;
     if (num_edges > kMaxEdges) return BCC_ERR_LIMIT;  // more edges than the fixed working arrays hold
-    if (bcc::records_smem_bytes(max_prims_per_env > 0 ? max_prims_per_env : 1, 4) > 200 * 1024) return BCC_ERR_LIMIT;
+    if (max_prims_per_env > ops->max_prims) return BCC_ERR_LIMIT;
+    if (bcc::records_smem_bytes(max_prims_per_env > 0 ? max_prims_per_env : 1, ops->num_env_groups,
+                                bcc::kRecordsWarps) > 200 * 1024)
+        return BCC_ERR_LIMIT;
     if (num_edges == 0 || num_envs == 0) return BCC_OK;
     if (!d_records && max_prims_per_env > 0) return BCC_ERR_INVALID_ARGUMENT;
     if (!d_env_offsets || !d_edges || !d_results) return BCC_ERR_INVALID_ARGUMENT;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BCC_ERR_CUDA;
     Scratch* s = nullptr;
-    if (setup_device(dev, s) != cudaSuccess) return BCC_ERR_CUDA;
+    if (setup_device(dev, ops, s) != cudaSuccess) return BCC_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     // Stale contents from the previous call: clear what must start at zero.
@@ -111,14 +119,14 @@ extern "C" bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records,
     a.swept = s->swept;
     a.table = s->table;
     a.row_edge = s->row_edge;
-    if (bcc::launch_steps(BCC_ROBOT_PANDA, a, st) != cudaSuccess) return BCC_ERR_CUDA;
+    if (ops->steps(a, st) != cudaSuccess) return BCC_ERR_CUDA;
     int total = 0;
     if (cudaMemcpyAsync(&total, s->offs + num_edges, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return BCC_ERR_CUDA;
     if (total < 0 || total > kMaxRows) return BCC_ERR_LIMIT;  // the edges need more samples than the arrays hold
     a.total_rows = total;
-    if (bcc::launch_prep(BCC_ROBOT_PANDA, a, st) != cudaSuccess) return BCC_ERR_CUDA;
+    if (ops->prep(a, st) != cudaSuccess) return BCC_ERR_CUDA;
 
     bcc::RecordsParams P{};
     P.records = reinterpret_cast<const float4*>(d_records);
@@ -134,7 +142,7 @@ extern "C" bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records,
     P.edge_self = s->edge_self;
     P.results = d_results;
     P.error_flag = s->error;
-    if (bcc::launch_check_records(BCC_ROBOT_PANDA, P, st) != cudaSuccess) return BCC_ERR_CUDA;
+    if (ops->check_records(P, st) != cudaSuccess) return BCC_ERR_CUDA;
     int flag = 0;
     if (cudaMemcpyAsync(&flag, s->error, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)

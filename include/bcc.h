@@ -158,7 +158,7 @@ int32_t bcc_work_counters(bcc_ctx* ctx, uint64_t* out, int32_t max_counters);
  * implicit device synchronisation and unbounded latency are not allowed, or a
  * host framework that owns all device memory through its own pool.  It makes
  * no cudaMalloc/cudaFree or other allocating call and needs no bcc_ctx; its
- * working buffers are fixed arrays inside the library (about 5 MB on every GPU
+ * working buffers are fixed arrays inside the library (about 9 MB on every GPU
  * that loads it, kept until the process exits).
  *   d_records / d_env_offsets: device copies of bcc_pack_envs' output
  *     (records 16-byte aligned); max_prims_per_env: its max_prims_per_env.
