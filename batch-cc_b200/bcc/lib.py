@@ -20,6 +20,11 @@ from .envs import BccEnvSoa
 HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(HERE, "libbcc.so")
 ROBOTS = {"panda": 0, "fetch": 1, "baxter": 2}
+
+
+def _rid(robot):
+    """bcc_robot id of a robot name (an int passes through unchanged)."""
+    return robot if isinstance(robot, int) else _rid(robot)
 ORDERS = {"plain": 0, "learned": 1}
 STATUS = {0: "BCC_OK", 1: "BCC_ERR_INVALID_ARGUMENT", 2: "BCC_ERR_CUDA", 3: "BCC_ERR_NO_ENVS",
           4: "BCC_ERR_TIMEOUT", 5: "BCC_ERR_NOT_SUPPORTED", 6: "BCC_ERR_LIMIT"}
@@ -138,7 +143,7 @@ class Checker:
         if out is None:
             out = np.zeros((E, self.num_envs), np.uint8)
         opts = make_opts(order, use_graph=graph, tile=tile)
-        st = lib().bcc_check(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        st = lib().bcc_check(self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                              E, resolution, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
                              ctypes.byref(opts))
         self._raise(st)
@@ -199,7 +204,7 @@ class Checker:
         edges = np.ascontiguousarray(edges, np.float32)
         losses = np.zeros(epochs, np.float32)
         pos = ctypes.c_float(0)
-        self._raise(lib().bcc_mlp_train(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        self._raise(lib().bcc_mlp_train(self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                         len(edges), resolution, int(num_samples), epochs, batch, ctypes.c_float(lr),
                                         ctypes.c_uint64(seed), losses.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                         ctypes.byref(pos)))
@@ -208,7 +213,7 @@ class Checker:
     def mlp_evaluate(self, edges, num_samples, seed=1, resolution=32, robot="panda"):
         edges = np.ascontiguousarray(edges, np.float32)
         m = np.zeros(5, np.float32)
-        self._raise(lib().bcc_mlp_evaluate(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        self._raise(lib().bcc_mlp_evaluate(self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                            len(edges), resolution, int(num_samples), ctypes.c_uint64(seed),
                                            m.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return dict(zip(("loss", "mispredict", "false_pos", "false_neg", "positive"), [float(v) for v in m]))
@@ -232,7 +237,7 @@ class Checker:
     def autotune(self, edges, order="plain", resolution=32, robot="panda"):
         edges = np.ascontiguousarray(edges, np.float32)
         c = (ctypes.c_int32 * 4)()
-        self._raise(lib().bcc_autotune(self._h, ROBOTS[robot], edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        self._raise(lib().bcc_autotune(self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                        len(edges), resolution, ORDERS[order], c))
         return dict(zip(self.CONFIG, list(c)))
 
@@ -240,7 +245,7 @@ class Checker:
                      order="plain", stream=0, tile=0, graph=False):
         """Device API: raw device pointers (e.g. torch tensors' data_ptr()), stream-ordered."""
         opts = make_opts(order, use_graph=graph, tile=tile)
-        st = lib().bcc_check_device(self._h, ROBOTS[robot], ctypes.c_void_p(d_edges_ptr), num_edges,
+        st = lib().bcc_check_device(self._h, _rid(robot), ctypes.c_void_p(d_edges_ptr), num_edges,
                                     resolution, ctypes.c_void_p(d_results_ptr), ctypes.byref(opts),
                                     ctypes.c_void_p(stream))
         self._raise(st)

@@ -33,6 +33,24 @@ UNIT = "edges/s"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
+def metric_of(name, N):
+    """The headline metric on the headline workload; the same quantity, named
+    for its robot and size, on the others."""
+    from bcc import workload
+    if name == WORKLOAD:
+        return METRIC
+    return "edges/sec (%s, %d envs) learned-ordered vs plain; verdict mismatches=0" % (workload.robot_of(name), N)
+
+
+def workload_name(name, N, E):
+    """Human-readable workload description (robot, sizes, size laws)."""
+    from bcc import workload
+    w = workload.WORKLOADS[name]
+    prims = "8 spheres, 8 cuboids, 4 cylinders" if w["prims"] == "fixed" else "U{%d..%d} primitives" % w["prims"]
+    edges = "uniform in the joint limits" if w["edge_law"] == "uniform" else "log-uniform 0.05-2.0 rad"
+    return "%s: %s, %d envs (%s) x %d edges (%s)" % (name, w["robot"], N, prims, E, edges)
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -125,31 +143,31 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
-def cpu_baseline(envs, edges, target_s=12.0):
+def cpu_baseline(envs, edges, robot="panda", target_s=12.0):
     """The CPU restatement of the reference algorithm (oracle, FP32, all host
     threads) on a bounded sample: all environments x the first edges."""
     from oracle import oracle as orc
     cores = os.cpu_count() or 1
     n_e = 100
     t0 = time.perf_counter()
-    orc.check(envs, edges[:n_e], precision=32, nthreads=cores)
+    orc.check(envs, edges[:n_e], precision=32, nthreads=cores, robot=robot)
     dt = time.perf_counter() - t0
     n_e2 = int(min(len(edges), max(n_e, n_e * target_s / max(dt, 1e-3))))
     t0 = time.perf_counter()
-    orc.check(envs, edges[:n_e2], precision=32, nthreads=cores)
+    orc.check(envs, edges[:n_e2], precision=32, nthreads=cores, robot=robot)
     dt = time.perf_counter() - t0
     return {"value": n_e2 * envs.num_envs / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": "%d envs x first %d edges of the workload (%.1f s), FP32 CPU restatement of the "
                       "reference algorithm (oracle/oracle.cpp), not VAMP" % (envs.num_envs, n_e2, dt)}
 
 
-def algorithmic_flops(envs, edges, sample):
+def algorithmic_flops(envs, edges, sample, robot="panda"):
     """Reference plain-order FLOPs per pair (oracle count), averaged over a seeded
     uniform sample of (edge, env) pairs, times all pairs."""
     from oracle import oracle as orc
     rng = np.random.default_rng(123)
     pairs = np.stack([rng.integers(0, len(edges), sample), rng.integers(0, envs.num_envs, sample)], 1)
-    fl, _ = orc.pair_flops(envs, edges, pairs)
+    fl, _ = orc.pair_flops(envs, edges, pairs, robot=robot)
     return float(fl.mean()) * len(edges) * envs.num_envs, float(fl.std() / np.sqrt(sample) / fl.mean())
 
 
@@ -157,27 +175,28 @@ def run_reference(args, world, rank):
     from bcc import workload
     if rank != 0:
         return
+    robot = workload.robot_of(args.workload)
     envs = workload.gen_envs(args.workload, args.envs, seed=0)
     edges = workload.gen_edges(args.workload, args.edges, seed=0)
     N, E = envs.num_envs, len(edges)
-    cfg = {"workload": "%s: panda, %d envs (U{8..64} primitives) x %d edges (log-uniform 0.05-2.0 rad)" % (
-        args.workload, N, E), "envs": N, "edges": E, "resolution": 32}
+    cfg = {"workload": workload_name(args.workload, N, E), "envs": N, "edges": E, "resolution": 32}
     if args.ref_path == "cuda":
         from oracle import ref
         if not ref.available():
             print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
             return
         for _ in range(args.warmup):
-            ref.time_panda(envs, edges, iters=1)
-        ms, _ = ref.time_panda(envs, edges, iters=args.steps)
+            ref.time_kernel(envs, edges, iters=1, robot=robot)
+        ms, _ = ref.time_kernel(envs, edges, iters=args.steps, robot=robot)
         val = N * E / (ms * 1e-3)
         t0 = time.perf_counter()
-        ref.check_panda(envs, edges)
+        ref.check(envs, edges, robot=robot)
         e2e_s = time.perf_counter() - t0
-        line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        line = {"metric": metric_of(args.workload, N), "value": val, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": cfg,
-                "impl": "reference", "ref_path": "reference CUDA kernel batch_cc_kernel<Panda> (oracle/_ref)",
+                "impl": "reference",
+                "ref_path": "reference CUDA kernel batch_cc_kernel<%s> (oracle/_ref)" % robot.capitalize(),
                 "e2e": {"value": N * E / e2e_s, "unit": UNIT,
                         "h2d_bytes_per_step": int(edges.nbytes), "d2h_bytes_per_step": N * E}}
         print(json.dumps(line))
@@ -187,14 +206,14 @@ def run_reference(args, world, rank):
     # Each step: a bounded sample (all envs x a fixed slice of edges), rotating slices.
     per_step = max(50, min(E, 400))
     for w in range(args.warmup):
-        orc.check(envs, edges[:50], precision=32, nthreads=cores)
+        orc.check(envs, edges[:50], precision=32, nthreads=cores, robot=robot)
     t_tot = 0.0
     done = 0
     for s in range(args.steps):
         lo = (s * per_step) % E
         sl = edges[lo:lo + per_step]
         t0 = time.perf_counter()
-        orc.check(envs, sl, precision=32, nthreads=cores)
+        orc.check(envs, sl, precision=32, nthreads=cores, robot=robot)
         t_tot += time.perf_counter() - t0
         done += len(sl) * N
     val = done / t_tot
@@ -202,7 +221,8 @@ def run_reference(args, world, rank):
     sample = "%d envs x %d edges per step, %d steps (%.1f s), FP32 CPU restatement of the reference " \
              "algorithm (oracle/oracle.cpp); the reference's VAMP CPU path is not vendored" % (
                  N, per_step, args.steps, t_tot)
-    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+    line = {"metric": metric_of(args.workload, N), "value": val, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "config": cfg, "impl": "reference",
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
@@ -219,21 +239,22 @@ def train_proposal(chk, args):
     chk.mlp_set_params(mlp.init_params(1000))
     losses, pos = chk.mlp_train(workload.gen_edges(args.workload, args.edges, seed=1000),
                                 num_samples=args.train_samples, epochs=args.train_epochs, batch=16384, lr=2e-3,
-                                seed=1000)
+                                seed=1000, robot=workload.robot_of(args.workload))
     return {"train_samples": args.train_samples, "epochs": args.train_epochs, "epoch_loss": [float(v) for v in losses],
             "train_positive_fraction": pos, "train_seconds": time.perf_counter() - t0,
             "data": "checker-labelled samples of %s environments/edges with seed 1000 (benchmark uses seed 0)" % (
                 args.workload)}
 
 
-def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev):
+def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev, robot="panda"):
     """Timed region: `steps` graph-captured (persistent-kernel) checks, L2 flushed
     between steps outside the timed events; then an untimed eager pass for the
     per-stage breakdown."""
     import torch
 
     def step(graph):
-        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream, graph=graph)
+        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream, graph=graph,
+                         robot=robot)
 
     for _ in range(warmup):
         step(True)
@@ -287,12 +308,13 @@ def run_ours(args, world, rank, local, dist):
     dev = local
     torch.cuda.set_device(dev)
     chk = Checker(dev)
+    robot = workload.robot_of(args.workload)
     proposal = train_proposal(chk, args)
     envs = workload.gen_envs(args.workload, args.envs, seed=0)
     edges = workload.gen_edges(args.workload, args.edges, seed=rank)
     N, E = envs.num_envs, len(edges)
     chk.upload(envs)
-    proposal.update(chk.mlp_evaluate(edges, 1 << 20, seed=7))
+    proposal.update(chk.mlp_evaluate(edges, 1 << 20, seed=7, robot=robot))
     chk.set_profiling(True)
     stream = torch.cuda.current_stream()
     d_edges = torch.from_numpy(edges).to(f"cuda:{dev}")
@@ -301,7 +323,7 @@ def run_ours(args, world, rank, local, dist):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
     # Autotuned launch configuration per order (untimed), on the first edges.
-    tuned = {o: chk.autotune(edges[:min(E, 2000)], order=o) for o in ("plain", "learned")}
+    tuned = {o: chk.autotune(edges[:min(E, 2000)], order=o, robot=robot) for o in ("plain", "learned")}
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -309,7 +331,8 @@ def run_ours(args, world, rank, local, dist):
     with ClockSampler(dev) as clk:
         for order in ("plain", "learned"):
             chk.set_launch_config(**tuned[order])
-            results[order] = time_order(chk, d_edges, d_res, E, order, stream, args.steps, args.warmup, flush, dev)
+            results[order] = time_order(chk, d_edges, d_res, E, order, stream, args.steps, args.warmup, flush, dev,
+                                        robot)
     torch.cuda.synchronize()
 
     def max_over_ranks(v):
@@ -325,22 +348,23 @@ def run_ours(args, world, rank, local, dist):
 
     # Verdict agreement of the two orders (must be identical), and work counters.
     chk.set_launch_config(**tuned["plain"])
-    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="plain", stream=stream.cuda_stream)
+    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="plain", stream=stream.cuda_stream, robot=robot)
     chk.set_launch_config(**tuned["learned"])
-    chk.check_device(d_edges.data_ptr(), E, d_res2.data_ptr(), order="learned", stream=stream.cuda_stream)
+    chk.check_device(d_edges.data_ptr(), E, d_res2.data_ptr(), order="learned", stream=stream.cuda_stream,
+                     robot=robot)
     torch.cuda.synchronize()
     mismatch = int((d_res != d_res2).sum().item())
     work = {}
     chk.set_profiling(True, counters=True)
     for order in ("plain", "learned"):
         chk.set_launch_config(**tuned[order])
-        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream)
+        chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order=order, stream=stream.cuda_stream, robot=robot)
         torch.cuda.synchronize()
         c = chk.work_counters()
         work[order] = {k: v / max(c["pairs"], 1) for k, v in c.items() if k != "pairs"}
         work[order]["pairs_walked"] = c["pairs"]
     chk.set_profiling(True)
-    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream)
+    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream, robot=robot)
     torch.cuda.synchronize()
     learned_rows = chk.last_learned_rows()
 
@@ -348,12 +372,12 @@ def run_ours(args, world, rank, local, dist):
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
     h_res = torch.empty((E, N), dtype=torch.uint8).pin_memory().numpy()
     chk.set_launch_config(**tuned[head])
-    chk.check(h_edges, out=h_res, order=head)
+    chk.check(h_edges, out=h_res, order=head, robot=robot)
     t_e2e = []
     for _ in range(max(3, min(args.steps, 5))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        chk.check(h_edges, out=h_res, order=head)
+        chk.check(h_edges, out=h_res, order=head, robot=robot)
         t_e2e.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(statistics.median(t_e2e))
     mlp_ms, mlp_tf = mlp_roofline(chk, dev)
@@ -361,11 +385,11 @@ def run_ours(args, world, rank, local, dist):
     if rank != 0:
         chk.close()
         return
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    line = {"metric": metric_of(args.workload, N), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": "%s: panda, %d envs (U{8..64} primitives) x %d edges (log-uniform 0.05-2.0 rad), "
-                                   "resolution 32, %s-ordered" % (args.workload, N, E, head),
+            "config": {"workload": "%s, resolution 32, %s-ordered" % (workload_name(args.workload, N, E), head),
                        "envs": N, "edges_per_gpu": E, "order": head,
                        "l2": "256 MB buffer written between timed steps (untimed)", "parallelism": "dp%d" % world},
             "orders": {o: {"value": world * N * E / (ms[o] * 1e-3), "ms_per_step": ms[o],
@@ -382,7 +406,7 @@ def run_ours(args, world, rank, local, dist):
     # algorithmic FLOPs of the reference plain order per launch / mean
     # CUDA-event duration of the launch.
     peak = measure_fp32_peak(dev)
-    flops, rel_err = algorithmic_flops(envs, edges, args.flop_sample)
+    flops, rel_err = algorithmic_flops(envs, edges, args.flop_sample, robot)
     chk_ms = statistics.mean(results["plain"][1])
     achieved = flops / (chk_ms * 1e-3) / 1e12
     line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -400,7 +424,7 @@ def run_ours(args, world, rank, local, dist):
                             "kernel": "mlp_forward_kernel (tcgen05, 4M rows)", "kernel_ms": mlp_ms,
                             "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst) of measured"}
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(envs, edges)
+        line["cpu_baseline"] = cpu_baseline(envs, edges, robot)
     chk.close()
     print(json.dumps(line))
 

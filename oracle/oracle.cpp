@@ -44,6 +44,8 @@
 #include <vector>
 
 #include "../include/bcc.h"
+#include "../batch-cc_b200/csrc/robot_baxter.h"
+#include "../batch-cc_b200/csrc/robot_fetch.h"
 #include "../batch-cc_b200/csrc/robot_panda.h"
 
 namespace {
@@ -107,8 +109,10 @@ inline void sample_q(const Disc& d, int dof, int lane, int round, float* q) {
 }
 
 // ---------------------------------------------------------------- kinematics
+// Tree FK from the robot tables: frame k+1 = frame parent(k) * F_k * J_k(q_k),
+// J = Rz (revolute) or Tz (prismatic); evaluated in T.
 template <class M, class T>
-void forward_kinematics(const float* qf, T (*c)[3]) {
+void tree_fk(const float* qf, T (*c)[3]) {
     T R[M::dof + 1][3][3];
     T p[M::dof + 1][3];
     for (int a = 0; a < 3; ++a) {
@@ -117,20 +121,28 @@ void forward_kinematics(const float* qf, T (*c)[3]) {
     }
     for (int k = 0; k < M::dof; ++k) {
         const double* F = M::joint_tf[k];
+        const int P = M::joint_parent[k];
         T A[3][3];
         for (int a = 0; a < 3; ++a) {
             for (int b = 0; b < 3; ++b)
-                A[a][b] = R[k][a][0] * T(F[0 * 4 + b]) + R[k][a][1] * T(F[1 * 4 + b]) +
-                          R[k][a][2] * T(F[2 * 4 + b]);
-            p[k + 1][a] = R[k][a][0] * T(F[3]) + R[k][a][1] * T(F[7]) + R[k][a][2] * T(F[11]) +
-                          p[k][a];
+                A[a][b] = R[P][a][0] * T(F[0 * 4 + b]) + R[P][a][1] * T(F[1 * 4 + b]) +
+                          R[P][a][2] * T(F[2 * 4 + b]);
+            p[k + 1][a] = R[P][a][0] * T(F[3]) + R[P][a][1] * T(F[7]) + R[P][a][2] * T(F[11]) +
+                          p[P][a];
         }
         T q = T(qf[k]);
-        T cq = std::cos(q), sq = std::sin(q);
-        for (int a = 0; a < 3; ++a) {
-            R[k + 1][a][0] = A[a][0] * cq + A[a][1] * sq;
-            R[k + 1][a][1] = A[a][1] * cq - A[a][0] * sq;
-            R[k + 1][a][2] = A[a][2];
+        if (M::joint_type[k] == 0) {
+            T cq = std::cos(q), sq = std::sin(q);
+            for (int a = 0; a < 3; ++a) {
+                R[k + 1][a][0] = A[a][0] * cq + A[a][1] * sq;
+                R[k + 1][a][1] = A[a][1] * cq - A[a][0] * sq;
+                R[k + 1][a][2] = A[a][2];
+            }
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                for (int b = 0; b < 3; ++b) R[k + 1][a][b] = A[a][b];
+                p[k + 1][a] += A[a][2] * q;
+            }
         }
     }
     for (int s = 0; s < M::num_spheres; ++s) {
@@ -138,6 +150,21 @@ void forward_kinematics(const float* qf, T (*c)[3]) {
         const double* l = M::sphere_local[s];
         for (int a = 0; a < 3; ++a)
             c[s][a] = R[f][a][0] * T(l[0]) + R[f][a][1] * T(l[1]) + R[f][a][2] * T(l[2]) + p[f][a];
+    }
+}
+
+// Sphere centres in T.  Where the reference evaluates the robot's FK in double
+// (Fetch, Baxter: `auto X = q * 0.5; sin(X)` promotes) and passes the centres
+// to the float tests, the FP32 mode does the same: double FK, rounded to float.
+template <class M, class T>
+void forward_kinematics(const float* qf, T (*c)[3]) {
+    if (M::fk_precision == 64 && sizeof(T) < sizeof(double)) {
+        double cd[M::num_spheres][3];
+        tree_fk<M, double>(qf, cd);
+        for (int s = 0; s < M::num_spheres; ++s)
+            for (int a = 0; a < 3; ++a) c[s][a] = T(cd[s][a]);
+    } else {
+        tree_fk<M, T>(qf, c);
     }
 }
 
@@ -294,14 +321,13 @@ double config_pen(const EnvView& e, const float* q) {
 // each sphere_environment_in_collision call (2 for the inflation + per tested
 // primitive 11 sphere / 28 capsule / 18 z-capsule / 33 cuboid / 24 z-cuboid,
 // stopping at the first hit), then 11 per self test; returns the verdict.
-constexpr double kFlopFK = 1150.0;
 constexpr double kFlopPrim[5] = {11.0, 28.0, 18.0, 33.0, 24.0};
 
 template <class M>
 bool config_flops(const EnvView& e, const float* q, double& flops) {
     float c[M::num_spheres][3];
     forward_kinematics<M, float>(q, c);
-    flops += kFlopFK;
+    flops += double(M::fk_flops);
     auto scan = [&](int s) {
         float x = c[s][0], y = c[s][1], z = c[s][2];
         float r = M::sphere_radius[s] + 0.005f;
@@ -438,12 +464,25 @@ int pen_impl(const bcc_env_soa* envs, const float* edges, int res, const int64_t
 
 }  // namespace
 
+// Runs f(Model{}) for the robot's model; `fallback` for an unknown robot.
+template <class R, class F>
+R with_robot(int robot, R fallback, F&& f) {
+    switch (robot) {
+        case BCC_ROBOT_PANDA: return f(bcc::PandaModel{});
+        case BCC_ROBOT_FETCH: return f(bcc::FetchModel{});
+        case BCC_ROBOT_BAXTER: return f(bcc::BaxterModel{});
+        default: return fallback;
+    }
+}
+
 extern "C" {
 
-int orc_robot_dof(int robot) { return robot == BCC_ROBOT_PANDA ? bcc::PandaModel::dof : -1; }
+int orc_robot_dof(int robot) {
+    return with_robot(robot, -1, [](auto m) { return decltype(m)::dof; });
+}
 
 int orc_robot_num_spheres(int robot) {
-    return robot == BCC_ROBOT_PANDA ? bcc::PandaModel::num_spheres : -1;
+    return with_robot(robot, -1, [](auto m) { return decltype(m)::num_spheres; });
 }
 
 int orc_edge_n(const float* start, const float* end, int dof, int resolution) {
@@ -458,52 +497,63 @@ int orc_edge_samples(const float* start, const float* end, int dof, int resoluti
     return d.n;
 }
 
-// Sphere centres [num_spheres][3] of a configuration, FP64 chain.
+// Sphere centres [num_spheres][3] of a configuration, FP64 tree FK.
 int orc_fk(int robot, const float* q, double* centres) {
-    if (robot != BCC_ROBOT_PANDA) return -1;
-    forward_kinematics<bcc::PandaModel, double>(q, (double(*)[3])centres);
-    return 0;
+    return with_robot(robot, -1, [&](auto m) {
+        using M = decltype(m);
+        forward_kinematics<M, double>(q, (double(*)[3])centres);
+        return 0;
+    });
 }
 
 // One configuration against one environment (literal fkcc semantics); 1 = collision.
 int orc_config_collides(const bcc_env_soa* envs, int env, int robot, const float* q, int precision) {
-    if (robot != BCC_ROBOT_PANDA) return -1;
-    auto views = make_views(envs);
-    return precision == 32 ? config_collides<bcc::PandaModel, float>(views[env], q)
-                           : config_collides<bcc::PandaModel, double>(views[env], q);
+    return with_robot(robot, -1, [&](auto m) {
+        using M = decltype(m);
+        auto views = make_views(envs);
+        return (int)(precision == 32 ? config_collides<M, float>(views[env], q)
+                                     : config_collides<M, double>(views[env], q));
+    });
 }
 
 double orc_config_pen(const bcc_env_soa* envs, int env, int robot, const float* q) {
-    if (robot != BCC_ROBOT_PANDA) return std::nan("");
-    auto views = make_views(envs);
-    return config_pen<bcc::PandaModel>(views[env], q);
+    return with_robot(robot, std::nan(""), [&](auto m) {
+        using M = decltype(m);
+        auto views = make_views(envs);
+        return config_pen<M>(views[env], q);
+    });
 }
 
 // Verdicts of every (env, edge) pair, results[edge][env]; precision 64 or 32.
 int orc_check(const bcc_env_soa* envs, int robot, const float* edges, int num_edges, int resolution,
               int precision, int nthreads, uint8_t* out) {
-    if (robot != BCC_ROBOT_PANDA) return -1;
-    return check_impl<bcc::PandaModel>(envs, edges, num_edges, resolution, precision, nthreads, out);
+    return with_robot(robot, -1, [&](auto m) {
+        using M = decltype(m);
+        return check_impl<M>(envs, edges, num_edges, resolution, precision, nthreads, out);
+    });
 }
 
 // FP64 penetration of listed (edge, env) pairs; arg = sample index k of the maximum.
 int orc_pair_pen(const bcc_env_soa* envs, int robot, const float* edges, int resolution,
                  const int64_t* pairs, int num_pairs, int nthreads, double* pen, int32_t* arg) {
-    if (robot != BCC_ROBOT_PANDA) return -1;
-    return pen_impl<bcc::PandaModel>(envs, edges, resolution, pairs, num_pairs, nthreads, pen, arg);
+    return with_robot(robot, -1, [&](auto m) {
+        using M = decltype(m);
+        return pen_impl<M>(envs, edges, resolution, pairs, num_pairs, nthreads, pen, arg);
+    });
 }
 
 // Algorithmic FLOPs (reference plain order) of listed (edge, env) pairs.
 int orc_pair_flops(const bcc_env_soa* envs, int robot, const float* edges, int resolution,
                    const int64_t* pairs, int num_pairs, int nthreads, double* flops, uint8_t* verdict) {
-    if (robot != BCC_ROBOT_PANDA) return -1;
-    using M = bcc::PandaModel;
-    auto views = make_views(envs);
-    parallel_for(num_pairs, nthreads, [&](int64_t k) {
-        int64_t e = pairs[2 * k], v = pairs[2 * k + 1];
-        flops[k] = pair_flops<M>(views[v], edges + e * 2 * M::dof, resolution, verdict + k);
+    return with_robot(robot, -1, [&](auto m) {
+        using M = decltype(m);
+        auto views = make_views(envs);
+        parallel_for(num_pairs, nthreads, [&](int64_t k) {
+            int64_t e = pairs[2 * k], v = pairs[2 * k + 1];
+            flops[k] = pair_flops<M>(views[v], edges + e * 2 * M::dof, resolution, verdict + k);
+        });
+        return 0;
     });
-    return 0;
 }
 
 }  // extern "C"

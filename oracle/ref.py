@@ -32,36 +32,38 @@ def lib():
         f32p = ctypes.POINTER(ctypes.c_float)
         u8p = ctypes.POINTER(ctypes.c_uint8)
         i32p = ctypes.POINTER(ctypes.c_int32)
-        L.ref_check_panda.argtypes = [vp, f32p, ctypes.c_int, ctypes.c_int, u8p, ctypes.c_int]
-        L.ref_time_panda.argtypes = [vp, f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, f32p, u8p]
+        L.ref_check.argtypes = [ctypes.c_int, vp, f32p, ctypes.c_int, ctypes.c_int, u8p, ctypes.c_int]
+        L.ref_time.argtypes = [ctypes.c_int, vp, f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, f32p, u8p]
         L.ref_probe_samples.argtypes = [f32p, ctypes.c_int, ctypes.c_int, f32p, i32p]
         _lib = L
     return _lib
 
 
-def check_panda(envset, edges, resolution=32, quiet=True):
-    """Verdicts [E, N] from batch_cc::batch_cc<Panda> (the reference public API)."""
+ROBOTS = {"panda": 0, "fetch": 1, "baxter": 2}
+
+
+def check(envset, edges, resolution=32, quiet=True, robot="panda"):
+    """Verdicts [E, N] from batch_cc::batch_cc<Robot> (the reference public API)."""
     edges = np.ascontiguousarray(edges, np.float32)
     E = edges.shape[0]
     out = np.zeros((E, envset.num_envs), np.uint8)
     soa = envset.as_ctypes()
-    rc = lib().ref_check_panda(ctypes.byref(soa), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), E,
-                               resolution, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), int(quiet))
+    rc = lib().ref_check(ROBOTS[robot], ctypes.byref(soa), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), E,
+                         resolution, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), int(quiet))
     if rc != 0:
         raise RuntimeError("reference batch_cc failed with CUDA error %d" % rc)
     return out
 
 
-def time_panda(envset, edges, resolution=32, iters=3):
+def time_kernel(envset, edges, resolution=32, iters=3, robot="panda"):
     """(mean kernel ms, verdicts [E, N]) of the reference kernel, CUDA-event timed."""
     edges = np.ascontiguousarray(edges, np.float32)
     E = edges.shape[0]
     out = np.zeros((E, envset.num_envs), np.uint8)
     ms = ctypes.c_float(0)
     soa = envset.as_ctypes()
-    rc = lib().ref_time_panda(ctypes.byref(soa), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), E,
-                              resolution, iters, ctypes.byref(ms),
-                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    rc = lib().ref_time(ROBOTS[robot], ctypes.byref(soa), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                        E, resolution, iters, ctypes.byref(ms), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
     if rc != 0:
         raise RuntimeError("reference kernel failed with CUDA error %d" % rc)
     return float(ms.value), out

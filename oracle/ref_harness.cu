@@ -4,16 +4,23 @@
 // This translation unit #includes the reference's src/batch_cc.cu unmodified
 // (compiled for sm_100a from the reference tree by oracle/Makefile, target
 // `ref`) and exposes:
-//   ref_check_panda    -- batch_cc::batch_cc<Panda>, the reference public API
+//   ref_check          -- batch_cc::batch_cc<Robot>, the reference public API
 //                         (src/batch_cc.hh:4-6), on environments rebuilt with
 //                         the reference shape constructors;
-//   ref_time_panda     -- the reference kernel batch_cc_kernel<Panda>
+//   ref_time           -- the reference kernel batch_cc_kernel<Robot>
 //                         (src/batch_cc.cu:74-133) on environments placed by the
 //                         reference's setup_environment_on_device, timed with
 //                         CUDA events;
 //   ref_probe_samples  -- batch_cc_kernel instantiated with a probe robot whose
 //                         fkcc records every configuration the kernel checks: the
 //                         reference's exact discretisation, as golden vectors.
+// Robot = Panda, Fetch or Baxter.  The reference's Fetch and Baxter check
+// functions (fkcc<Fetch> src/utils.cuh:10382, fkcc<Baxter> :24994) have the
+// three-argument signature while batch_cc_kernel calls the five-argument one,
+// and their batch_cc instantiations are commented out (src/batch_cc.cu:341-342);
+// this file adds five-argument specialisations that forward to the reference's
+// own three-argument functions, and the two instantiations, without touching
+// the reference sources.
 // Headers the reference received transitively through Eigen (std::memcpy).
 #include <unistd.h>
 
@@ -124,6 +131,26 @@ std::vector<std::array<std::array<float, DOF>, 2>> build_edges(const float* edge
 
 }  // namespace
 
+// Five-argument entry points of the reference's Fetch / Baxter check functions.
+template <>
+__device__ __forceinline__ bool ppln::collision::fkcc<ppln::robots::Fetch>(volatile float* q,
+                                                                           ppln::collision::Environment<float>* env,
+                                                                           int tid, int, int) {
+    return ppln::collision::fkcc<ppln::robots::Fetch>(q, env, tid);
+}
+template <>
+__device__ __forceinline__ bool ppln::collision::fkcc<ppln::robots::Baxter>(volatile float* q,
+                                                                            ppln::collision::Environment<float>* env,
+                                                                            int tid, int, int) {
+    return ppln::collision::fkcc<ppln::robots::Baxter>(q, env, tid);
+}
+template void batch_cc::batch_cc<ppln::robots::Fetch>(
+    std::vector<ppln::collision::Environment<float>>&,
+    std::vector<std::array<typename ppln::robots::Fetch::Configuration, 2>>&, int, std::vector<bool>&);
+template void batch_cc::batch_cc<ppln::robots::Baxter>(
+    std::vector<ppln::collision::Environment<float>>&,
+    std::vector<std::array<typename ppln::robots::Baxter::Configuration, 2>>&, int, std::vector<bool>&);
+
 // Probe fkcc: records the configuration and reports "free" so every round runs.
 template <>
 __device__ __forceinline__ bool ppln::collision::fkcc<ProbeRobot>(volatile float* config,
@@ -137,16 +164,16 @@ __device__ __forceinline__ bool ppln::collision::fkcc<ProbeRobot>(volatile float
     return true;
 }
 
-extern "C" {
+namespace {
 
-int ref_check_panda(const bcc_env_soa* envs, const float* edges, int E, int resolution, uint8_t* out,
-                    int quiet) {
+template <class Robot>
+int check_robot(const bcc_env_soa* envs, const float* edges, int E, int resolution, uint8_t* out, int quiet) {
     auto h_envs = build_envs(envs);
-    auto h_edges = build_edges<7>(edges, E);
+    auto h_edges = build_edges<Robot::dimension>(edges, E);
     std::vector<bool> results((size_t)E * envs->num_envs);
     {
         QuietStdout q(quiet != 0);
-        batch_cc::batch_cc<ppln::robots::Panda>(h_envs, h_edges, resolution, results);
+        batch_cc::batch_cc<Robot>(h_envs, h_edges, resolution, results);
     }
     for (size_t i = 0; i < results.size(); ++i) out[i] = results[i] ? 1 : 0;
     return (int)cudaGetLastError();
@@ -154,11 +181,13 @@ int ref_check_panda(const bcc_env_soa* envs, const float* edges, int E, int reso
 
 // Reference kernel on reference-placed environments; returns mean kernel ms
 // over `iters` launches (after one warm-up), verdicts of the last launch.
-int ref_time_panda(const bcc_env_soa* envs, const float* edges, int E, int resolution, int iters,
-                   float* ms_out, uint8_t* out) {
+template <class Robot>
+int time_robot(const bcc_env_soa* envs, const float* edges, int E, int resolution, int iters, float* ms_out,
+               uint8_t* out) {
     using EnvF = ppln::collision::Environment<float>;
     auto h_envs = build_envs(envs);
     const int N = envs->num_envs;
+    const size_t edge_bytes = sizeof(float) * 2 * Robot::dimension * (size_t)E;
     std::vector<EnvF*> d_envs(N, nullptr);
     std::vector<void*> d_blobs;
     for (int i = 0; i < N; ++i) batch_cc::setup_environment_on_device(d_envs[i], h_envs[i], d_blobs);
@@ -167,19 +196,17 @@ int ref_time_panda(const bcc_env_soa* envs, const float* edges, int E, int resol
     bool* d_res = nullptr;
     cudaMalloc(&d_envs_ptr, sizeof(EnvF*) * N);
     cudaMemcpy(d_envs_ptr, d_envs.data(), sizeof(EnvF*) * N, cudaMemcpyHostToDevice);
-    cudaMalloc(&d_edges, sizeof(float) * 14 * (size_t)E);
-    cudaMemcpy(d_edges, edges, sizeof(float) * 14 * (size_t)E, cudaMemcpyHostToDevice);
+    cudaMalloc(&d_edges, edge_bytes);
+    cudaMemcpy(d_edges, edges, edge_bytes, cudaMemcpyHostToDevice);
     cudaMalloc(&d_res, (size_t)N * E);
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     const long long blocks = (long long)N * E;
-    batch_cc::batch_cc_kernel<ppln::robots::Panda><<<(unsigned)blocks, 32>>>(d_envs_ptr, d_edges, N, E, d_res,
-                                                                             resolution);
+    batch_cc::batch_cc_kernel<Robot><<<(unsigned)blocks, 32>>>(d_envs_ptr, d_edges, N, E, d_res, resolution);
     cudaEventRecord(a);
     for (int it = 0; it < iters; ++it)
-        batch_cc::batch_cc_kernel<ppln::robots::Panda><<<(unsigned)blocks, 32>>>(d_envs_ptr, d_edges, N, E,
-                                                                                 d_res, resolution);
+        batch_cc::batch_cc_kernel<Robot><<<(unsigned)blocks, 32>>>(d_envs_ptr, d_edges, N, E, d_res, resolution);
     cudaEventRecord(b);
     cudaEventSynchronize(b);
     float ms = 0;
@@ -194,6 +221,34 @@ int ref_time_panda(const bcc_env_soa* envs, const float* edges, int E, int resol
     cudaFree(d_edges);
     cudaFree(d_res);
     return err;
+}
+
+}  // namespace
+
+extern "C" {
+
+// robot: BCC_ROBOT_PANDA / _FETCH / _BAXTER; -1 for an unknown robot.
+int ref_check(int robot, const bcc_env_soa* envs, const float* edges, int E, int resolution, uint8_t* out,
+              int quiet) {
+    switch (robot) {
+        case BCC_ROBOT_PANDA: return check_robot<ppln::robots::Panda>(envs, edges, E, resolution, out, quiet);
+        case BCC_ROBOT_FETCH: return check_robot<ppln::robots::Fetch>(envs, edges, E, resolution, out, quiet);
+        case BCC_ROBOT_BAXTER: return check_robot<ppln::robots::Baxter>(envs, edges, E, resolution, out, quiet);
+        default: return -1;
+    }
+}
+
+int ref_time(int robot, const bcc_env_soa* envs, const float* edges, int E, int resolution, int iters,
+             float* ms_out, uint8_t* out) {
+    switch (robot) {
+        case BCC_ROBOT_PANDA:
+            return time_robot<ppln::robots::Panda>(envs, edges, E, resolution, iters, ms_out, out);
+        case BCC_ROBOT_FETCH:
+            return time_robot<ppln::robots::Fetch>(envs, edges, E, resolution, iters, ms_out, out);
+        case BCC_ROBOT_BAXTER:
+            return time_robot<ppln::robots::Baxter>(envs, edges, E, resolution, iters, ms_out, out);
+        default: return -1;
+    }
 }
 
 // Configurations the reference kernel checks: out [E][32][16][7] (lane, round),

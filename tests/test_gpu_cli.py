@@ -55,6 +55,6 @@ def test_cli_matches_oracle_and_reference(tmp_path, args):
     n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, orc.check(envs, edges))
     assert len(bad) == 0
     if ref.available():
-        want = ref.check_panda(envs, edges)
+        want = ref.check(envs, edges)
         n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, want)
         assert len(bad) == 0

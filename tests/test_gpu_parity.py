@@ -13,28 +13,33 @@ from bcc.workload import make_capsules, make_cuboids, make_spheres
 from oracle import oracle as orc
 from oracle import ref
 
+import cases
+from bcc import lib as bcclib
+
 pytestmark = pytest.mark.gpu
 
 TOL = orc.ADJUDICATION_TOL_M  # 1e-5 m
 
 
-def assert_parity(envs, edges, got, want, label):
-    n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, want, tol=TOL)
+def assert_parity(envs, edges, got, want, label, robot="panda"):
+    n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, want, tol=TOL, robot=robot)
     assert len(bad) == 0, "%s: %d mismatches, %d out of tolerance, e.g. (edge, env) %s" % (
         label, n_mis, len(bad), bad[:5].tolist())
     return n_mis
 
 
 @pytest.mark.parametrize("name,nenv,nedge,seed", [
-    ("plain", 16, 200, 1), ("uneven", 40, 300, 2), ("uneven", 7, 513, 3), ("stress", 25, 150, 4)])
+    ("plain", 16, 200, 1), ("uneven", 40, 300, 2), ("uneven", 7, 513, 3), ("stress", 25, 150, 4),
+    ("multi_fetch", 16, 150, 5), ("multi_baxter", 12, 120, 6)])
 def test_checker_matches_oracle(checker, name, nenv, nedge, seed):
+    robot = workload.robot_of(name)
     envs = workload.gen_envs(name, nenv, seed=seed)
     edges = workload.gen_edges(name, nedge, seed=seed)
     checker.upload(envs)
-    got = checker.check(edges)
-    want = orc.check(envs, edges, precision=64)
+    got = checker.check(edges, robot=robot)
+    want = orc.check(envs, edges, precision=64, robot=robot)
     assert got.shape == want.shape
-    assert_parity(envs, edges, got, want, name)
+    assert_parity(envs, edges, got, want, name, robot)
 
 
 def test_edge_cases(checker):
@@ -77,6 +82,41 @@ def test_known_answer_contact(checker):
     assert got.tolist() == [[0, 1]]
 
 
+@pytest.mark.parametrize("robot", ["fetch", "baxter"])
+def test_overhanging_leaf_needs_the_bound_to_hit_somewhere(checker, robot):
+    """Leaves sticking out of their bound: a leaf hit counts only when the
+    bound hits SOME primitive at that sample (reference gate semantics), also
+    when that primitive is not the one the leaf hits -- through the grid
+    kernel, the persistent kernel and the records kernel."""
+    import ctypes
+
+    import torch
+
+    from test_zz_no_alloc import _noalloc_fn, _pack
+
+    q, envs, want = cases.overhang_case(robot)
+    edge = np.ascontiguousarray(np.stack([q, q])[None])
+    checker.upload(envs)
+    old = checker.launch_config()
+    try:
+        for warps, persistent in ((4, 0), (8, 1)):
+            checker.set_launch_config(warps=warps, persistent=persistent)
+            assert checker.check(edge, robot=robot)[0].tolist() == want.tolist(), (warps, persistent)
+    finally:
+        checker.set_launch_config(**old)
+    # the allocation-free entry point (records kernel)
+    rec, off, max_prims = _pack(envs)
+    d_rec, d_off = torch.from_numpy(rec).cuda(), torch.from_numpy(off).cuda()
+    d_edges = torch.from_numpy(edge).cuda()
+    d_res = torch.full((1, 3), 7, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    st = _noalloc_fn()(bcclib.ROBOTS[robot], d_rec.data_ptr(), d_off.data_ptr(), 3, max_prims, d_edges.data_ptr(),
+                       1, 32, d_res.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0
+    torch.cuda.synchronize()
+    assert d_res.cpu().numpy()[0].tolist() == want.tolist()
+
+
 def test_results_layout_and_env_permutation(checker):
     envs = workload.gen_envs("uneven", 30, seed=12)
     edges = workload.gen_edges("uneven", 100, seed=12)
@@ -112,7 +152,7 @@ def test_errors_are_reported(checker):
     with pytest.raises(BccError):
         checker.check(workload.gen_edges("plain", 4, seed=0), resolution=0)
     with pytest.raises(BccError):
-        checker.check(workload.gen_edges("plain", 4, seed=0), robot="fetch")
+        checker.check(workload.gen_edges("plain", 4, seed=0), robot=7)  # no such robot
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference harness not built")
@@ -135,16 +175,18 @@ def test_reference_kernel_sample_set_is_the_oracles():
 
 
 @pytest.mark.skipif(not ref.available(), reason="reference harness not built")
-@pytest.mark.parametrize("name,nenv,nedge,seed", [("plain", 12, 150, 31), ("uneven", 30, 200, 32)])
+@pytest.mark.parametrize("name,nenv,nedge,seed", [("plain", 12, 150, 31), ("uneven", 30, 200, 32),
+                                                  ("multi_fetch", 12, 100, 33), ("multi_baxter", 10, 80, 34)])
 def test_checker_matches_reference_cuda_path(checker, name, nenv, nedge, seed):
+    robot = workload.robot_of(name)
     envs = workload.gen_envs(name, nenv, seed=seed)
     edges = workload.gen_edges(name, nedge, seed=seed)
-    want = ref.check_panda(envs, edges)
+    want = ref.check(envs, edges, robot=robot)
     checker.upload(envs)
-    got = checker.check(edges)
-    assert_parity(envs, edges, got, want, "vs reference CUDA")
+    got = checker.check(edges, robot=robot)
+    assert_parity(envs, edges, got, want, "vs reference CUDA", robot)
     # and the oracle against the reference (pins the oracle itself)
-    assert_parity(envs, edges, orc.check(envs, edges), want, "oracle vs reference CUDA")
+    assert_parity(envs, edges, orc.check(envs, edges, robot=robot), want, "oracle vs reference CUDA", robot)
 
 
 def test_full_size_properties(checker):

@@ -10,22 +10,84 @@ from bcc import EnvSet, workload
 from bcc.workload import make_capsules, make_cuboids, make_spheres
 from oracle import oracle as orc
 
+import cases
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def test_fk_matches_reference_generated_code():
-    """Sphere centres of the chain tables == the reference's generated fkcc<Panda>
-    FK expressions evaluated in FP64 (tests/golden/panda_fk_generated.json)."""
-    g = json.load(open(os.path.join(GOLDEN, "panda_fk_generated.json")))
+# Largest difference between the tables' FK and the reference's generated FK
+# expressions: FP64 rounding for Panda and Fetch; Baxter's generated FK
+# multiplies quaternions whose constants carry 7 digits, so it is rigid only to
+# about 2e-7 m and the fitted tree matches it to that level.
+FK_TOL = {"panda": 1e-12, "fetch": 1e-12, "baxter": 5e-7}
+
+
+@pytest.mark.parametrize("robot", ["panda", "fetch", "baxter"])
+def test_fk_matches_reference_generated_code(robot):
+    """Sphere centres of the robot tables == the reference's generated fkcc<Robot>
+    FK expressions evaluated in FP64 (tests/golden/<robot>_fk_generated.json)."""
+    g = json.load(open(os.path.join(GOLDEN, robot + "_fk_generated.json")))
     assert len(g["cases"]) >= 32
+    src = g.get("src_of_sphere")
     worst = 0.0
     for c in g["cases"]:
         q = np.array(c["q"], np.float32)
         assert np.array_equal(q.astype(np.float64), np.array(c["q"]))
-        got = orc.fk(q)
+        got = orc.fk(q, robot)
         want = np.array(c["centres"])
-        worst = max(worst, float(np.abs(got - want).max()))
-    assert worst < 1e-12, worst
+        if src is None:
+            worst = max(worst, float(np.abs(got - want).max()))
+        else:
+            idx = np.array(src)
+            has = idx >= 0  # synthetic bounds have no generated counterpart
+            assert sorted(set(idx[has].tolist())) == list(range(len(want)))
+            worst = max(worst, float(np.abs(got[has] - want[idx[has]]).max()))
+    assert worst < FK_TOL[robot], worst
+
+
+@pytest.mark.parametrize("robot", ["panda", "fetch", "baxter"])
+def test_leaves_stay_inside_the_padded_bound(robot):
+    """Every environment leaf lies inside its group's bound grown by the group's
+    cull pad, at any configuration (the checker culls with the padded bound),
+    and a leaf outside the plain bound is one of the group's listed
+    overhanging leaves.  Leaves within 1 um of the bound count as inside
+    (Panda's stick out by 4.4e-9 m; the cull adds a 1e-4 m margin)."""
+    m = cases.robot_model(robot)
+    r = np.array([s["r"] for s in m["spheres"]])
+    rng = np.random.default_rng(17)
+    s_m, s_a = workload.LIMITS[robot]
+    for _ in range(300):
+        q = (rng.uniform(-0.2, 1.2, len(s_m)) * s_m + s_a).astype(np.float32)
+        c = orc.fk(q, robot)
+        for g in m["env_groups"]:
+            b = g["bound"]
+            pad = g.get("cull_pad", 0.0)
+            for i, l in enumerate(g["leaves"]):
+                out = np.linalg.norm(c[l] - c[b]) + r[l] - r[b]
+                assert out <= pad + 1e-6, (g["link"], l, out, pad)
+                if out > 1e-6:
+                    assert i < g.get("over_count", 0), (g["link"], l, out)
+
+
+@pytest.mark.parametrize("robot", ["fetch", "baxter"])
+def test_overhang_case_separates_gate_semantics(robot):
+    """The overhang known answer: the reference's semantics (oracle) give
+    {A} free, {B} free, {A, B} colliding, and gating each leaf on its bound
+    hitting the same primitive would call {A, B} free."""
+    q, envs, want = cases.overhang_case(robot)
+    assert want.tolist() == [0, 0, 1]
+    v = orc.check(envs, np.stack([q, q])[None], robot=robot)
+    assert v[0].tolist() == [0, 0, 1]
+    # per-primitive gating on {A, B}
+    m = cases.robot_model(robot)
+    r = np.array([s["r"] for s in m["spheres"]]) + cases.INFLATE
+    c = orc.fk(q, robot)
+    obst = envs.env(2)["spheres"]  # the {A, B} environment's two spheres
+    assert len(obst) == 2
+    hit = lambda i, o: np.linalg.norm(c[i] - o[:3]) < r[i] + o[3]
+    per_prim = any(hit(g["bound"], o) and any(hit(l, o) for l in g["leaves"])
+                   for g in m["env_groups"] for o in obst)
+    assert not per_prim
 
 
 def test_discretisation_rules():
@@ -129,12 +191,14 @@ def test_cylinders_are_never_tested():
     assert np.array_equal(v[:, 0], v[:, 1])
 
 
-def test_fp32_and_fp64_oracles_agree_up_to_contact():
-    envs = workload.gen_envs("uneven", 24, seed=11)
-    edges = workload.gen_edges("uneven", 120, seed=11)
-    v64 = orc.check(envs, edges, precision=64)
-    v32 = orc.check(envs, edges, precision=32)
-    n, adj, bad = orc.adjudicate(envs, edges, v32, v64)
+@pytest.mark.parametrize("name,nenv,nedge", [("uneven", 24, 120), ("multi_fetch", 10, 60), ("multi_baxter", 8, 50)])
+def test_fp32_and_fp64_oracles_agree_up_to_contact(name, nenv, nedge):
+    robot = workload.robot_of(name)
+    envs = workload.gen_envs(name, nenv, seed=11)
+    edges = workload.gen_edges(name, nedge, seed=11)
+    v64 = orc.check(envs, edges, precision=64, robot=robot)
+    v32 = orc.check(envs, edges, precision=32, robot=robot)
+    n, adj, bad = orc.adjudicate(envs, edges, v32, v64, robot=robot)
     assert len(bad) == 0
 
 
@@ -185,7 +249,7 @@ def test_leaf_list_matches_model():
     assert leaves == sorted(LEAVES)
 
 
-@pytest.mark.parametrize("name", ["plain", "uneven", "stress"])
+@pytest.mark.parametrize("name", ["plain", "uneven", "stress", "multi_fetch", "multi_baxter"])
 def test_workload_generators_are_seeded(name):
     a = workload.gen_envs(name, 5, seed=9)
     b = workload.gen_envs(name, 5, seed=9)
@@ -194,5 +258,6 @@ def test_workload_generators_are_seeded(name):
     e1 = workload.gen_edges(name, 50, seed=9)
     e2 = workload.gen_edges(name, 50, seed=9)
     assert np.array_equal(e1, e2)
-    s_m, s_a = workload.LIMITS["panda"]
+    s_m, s_a = workload.LIMITS[workload.robot_of(name)]
+    assert e1.shape[2] == len(s_m)
     assert np.all(e1 >= s_a - 1e-5) and np.all(e1 <= s_a + s_m + 1e-5)

@@ -44,10 +44,13 @@ def _pack(envs):
     return rec, off, mp.value
 
 
-def test_noalloc_matches_bcc_check_twice():
+@pytest.mark.parametrize("name,nenv,nedge", [("uneven", 24, 96), ("multi_fetch", 12, 40), ("multi_baxter", 10, 40)])
+def test_noalloc_matches_bcc_check_twice(name, nenv, nedge):
     import torch
 
-    envs = workload.gen_envs("uneven", 24, seed=41)
+    robot = workload.robot_of(name)
+    rid = bcclib.ROBOTS[robot]
+    envs = workload.gen_envs(name, nenv, seed=41)
     rec, off, max_prims = _pack(envs)
     d_rec = torch.from_numpy(rec).cuda()
     d_off = torch.from_numpy(off).cuda()
@@ -55,18 +58,18 @@ def test_noalloc_matches_bcc_check_twice():
     chk = bcclib.Checker(0)
     chk.upload(envs)
     for call, seed in enumerate((42, 43)):
-        edges = workload.gen_edges("uneven", 96, seed=seed)
-        want = chk.check(edges)
+        edges = workload.gen_edges(name, nedge, seed=seed)
+        want = chk.check(edges, robot=robot)
         d_edges = torch.from_numpy(edges).cuda()
         d_res = torch.full((len(edges), envs.num_envs), 7, dtype=torch.uint8, device="cuda")
         torch.cuda.synchronize()
-        st = fn(0, d_rec.data_ptr(), d_off.data_ptr(), envs.num_envs, max_prims, d_edges.data_ptr(), len(edges),
+        st = fn(rid, d_rec.data_ptr(), d_off.data_ptr(), envs.num_envs, max_prims, d_edges.data_ptr(), len(edges),
                 32, d_res.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
         assert st == 0, "call %d returned status %d" % (call, st)
         torch.cuda.synchronize()
         got = d_res.cpu().numpy()
         assert set(np.unique(got)) <= {0, 1}
-        n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, want)
+        n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, want, robot=robot)
         assert len(bad) == 0, "call %d: %d mismatches beyond 1e-5 m of contact" % (call, len(bad))
     chk.close()
 
