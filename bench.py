@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--flop-sample", type=int, default=20000)
+    p.add_argument("--profile-order", default=None, choices=["plain", "learned"],
+                   help="profiling run: only `--steps` eager checks in this order (launch config of the "
+                        "library's defaults, MLP at its seeded initialisation), no training, tuning or baselines")
     p.add_argument("--envs", type=int, default=None, help="smaller case for profiling")
     p.add_argument("--edges", type=int, default=None, help="smaller case for profiling")
     return p.parse_args()
@@ -300,6 +303,29 @@ def mlp_roofline(chk, dev, rows=1 << 22, reps=5):
     return ms, flops / (ms * 1e-3) / 1e12
 
 
+def run_profile(args, local):
+    """The check alone, for ncu: `warmup` + `steps` eager checks of the workload."""
+    import torch
+    from bcc import mlp, workload
+    from bcc.lib import Checker
+
+    torch.cuda.set_device(local)
+    robot = workload.robot_of(args.workload)
+    chk = Checker(local)
+    envs = workload.gen_envs(args.workload, args.envs, seed=0)
+    edges = workload.gen_edges(args.workload, args.edges, seed=0)
+    chk.upload(envs)
+    if args.profile_order == "learned":
+        chk.mlp_set_params(mlp.init_params(1000))
+    for _ in range(args.warmup + args.steps):
+        chk.check(edges, order=args.profile_order, robot=robot)
+    torch.cuda.synchronize()
+    chk.close()
+    print(json.dumps({"profile": args.profile_order, "workload": workload_name(args.workload, envs.num_envs,
+                                                                               len(edges)),
+                      "checks": args.warmup + args.steps}))
+
+
 def run_ours(args, world, rank, local, dist):
     import torch
     from bcc import workload
@@ -435,6 +461,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.profile_order:
+            run_profile(args, local)
         else:
             run_ours(args, world, rank, local, dist)
     finally:
