@@ -24,7 +24,7 @@ ROBOTS = {"panda": 0, "fetch": 1, "baxter": 2}
 
 def _rid(robot):
     """bcc_robot id of a robot name (an int passes through unchanged)."""
-    return robot if isinstance(robot, int) else _rid(robot)
+    return robot if isinstance(robot, int) else ROBOTS[robot]
 ORDERS = {"plain": 0, "learned": 1}
 STATUS = {0: "BCC_OK", 1: "BCC_ERR_INVALID_ARGUMENT", 2: "BCC_ERR_CUDA", 3: "BCC_ERR_NO_ENVS",
           4: "BCC_ERR_TIMEOUT", 5: "BCC_ERR_NOT_SUPPORTED", 6: "BCC_ERR_LIMIT"}

@@ -120,3 +120,10 @@ def test_checker_without_gpu_fails_loudly():
         pytest.skip("GPU present")
     with pytest.raises(bcclib.BccError):
         bcclib.Checker(0)
+
+
+def test_robot_ids_of_the_binding():
+    from bcc.lib import ROBOTS, _rid
+    assert [_rid(r) for r in ("panda", "fetch", "baxter")] == [0, 1, 2]
+    assert _rid(7) == 7  # ids pass through (an unknown one is the library's to reject)
+    assert ROBOTS == {"panda": 0, "fetch": 1, "baxter": 2}
