@@ -67,8 +67,11 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--flop-sample", type=int, default=20000)
     p.add_argument("--profile-order", default=None, choices=["plain", "learned"],
-                   help="profiling run: only `--steps` eager checks in this order (launch config of the "
-                        "library's defaults, MLP at its seeded initialisation), no training, tuning or baselines")
+                   help="profiling run: only `--warmup` + `--steps` eager checks in this order (launch config "
+                        "--profile-launch, MLP at its seeded initialisation), no training, tuning or baselines")
+    p.add_argument("--profile-launch", default="128,4,0",
+                   help="edges per CTA, warps per CTA, persistent (0/1) of a profiling run; the default is the "
+                        "configuration the autotuner picks for the plain order of the uneven workload")
     p.add_argument("--envs", type=int, default=None, help="smaller case for profiling")
     p.add_argument("--edges", type=int, default=None, help="smaller case for profiling")
     return p.parse_args()
@@ -317,13 +320,15 @@ def run_profile(args, local):
     chk.upload(envs)
     if args.profile_order == "learned":
         chk.mlp_set_params(mlp.init_params(1000))
+    tile, warps, persistent = (int(v) for v in args.profile_launch.split(","))
+    chk.set_launch_config(edges_per_cta=tile, warps=warps, persistent=persistent)
     for _ in range(args.warmup + args.steps):
         chk.check(edges, order=args.profile_order, robot=robot)
     torch.cuda.synchronize()
     chk.close()
     print(json.dumps({"profile": args.profile_order, "workload": workload_name(args.workload, envs.num_envs,
                                                                                len(edges)),
-                      "checks": args.warmup + args.steps}))
+                      "checks": args.warmup + args.steps, "launch": args.profile_launch}))
 
 
 def run_ours(args, world, rank, local, dist):
