@@ -483,11 +483,12 @@ bcc_status pack(bcc_ctx* ctx, const bcc_env_soa* envs, std::vector<Rec>& recs, s
 }
 
 // Device arena: per environment a blob of its rounded-box records followed by
-// its interval-mask cull tables, and a 2 x float4 header.
+// its interval-mask cull tables, and a 2 x float4 header.  The check kernel
+// stages the records into shared memory and reads the mask tables through L1.
 struct Arena {
     std::vector<float> blob;     // concatenated blobs (float words, 16-byte granules)
     std::vector<float> hdr;      // [N][8]
-    size_t max_blob_bytes = 0;
+    size_t max_record_bytes = 0;
 };
 
 void build_arena(const std::vector<Rec>& recs, const std::vector<int>& off, Arena& A) {
@@ -542,8 +543,7 @@ void build_arena(const std::vector<Rec>& recs, const std::vector<int>& off, Aren
             A.blob.resize(at + words);
             std::memcpy(&A.blob[at], m.data(), m.size() * sizeof(uint64_t));
         }
-        const size_t bytes = (A.blob.size() - start) * sizeof(float);
-        A.max_blob_bytes = std::max(A.max_blob_bytes, bytes);
+        A.max_record_bytes = std::max(A.max_record_bytes, (size_t)np * sizeof(Rec));
         const uint32_t off16 = (uint32_t)(start / 4);  // float4 units
         const uint32_t shape = (uint32_t)np | ((uint32_t)W << 16);
         float* h = &A.hdr[(size_t)i * 8];
@@ -587,9 +587,9 @@ bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
     const int N = envs->num_envs;
     Arena A;
     build_arena(recs, off, A);
-    const size_t blob_smem = (A.max_blob_bytes + 15) & ~(size_t)15;
+    const size_t blob_smem = (A.max_record_bytes + 15) & ~(size_t)15;
     if (blob_smem > 160 * 1024)
-        return fail(ctx, BCC_ERR_LIMIT, "an environment's primitives do not fit shared-memory staging (max ~1000)");
+        return fail(ctx, BCC_ERR_LIMIT, "an environment's primitives do not fit shared-memory staging (max 2048)");
     if (A.blob.size() / 4 > 0xffffffffull) return fail(ctx, BCC_ERR_LIMIT, "environment arena too large");
     BCC_CUDA(ctx, cudaSetDevice(ctx->device));
     BCC_CUDA(ctx, ctx->blobs.ensure(A.blob.size() * sizeof(float)));

@@ -73,10 +73,11 @@ cudaError_t launch_scan(const int* steps, int E, int* offs, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------------ sizing
-// Dynamic shared memory of a check CTA: the largest environment blob plus,
-// per warp, a (primitive, link) pair list of max_prims x groups entries.
+// Dynamic shared memory of a check CTA: the largest environment's records plus,
+// per warp, a (primitive, link) pair list of max_prims x groups entries, at
+// most kPairCap.
 size_t check_smem_bytes(int max_prims, int groups, size_t blob_smem, int warps) {
-    const size_t ppw = (size_t)((max_prims * groups + 7) & ~7);
+    const size_t ppw = (size_t)std::min((max_prims * groups + 7) & ~7, kPairCap);
     return blob_smem + (size_t)warps * ppw * sizeof(uint16_t);
 }
 

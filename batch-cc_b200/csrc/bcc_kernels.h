@@ -24,7 +24,7 @@ struct CheckParams {
     int num_envs;
     int num_edges;
     int max_prims;           // max primitives of one env (pair-list sizing)
-    size_t blob_smem;        // bytes of the largest env blob (16-byte multiple)
+    size_t blob_smem;        // bytes of the largest env's records (16-byte multiple)
     int pairs_per_warp;
     int edges_per_cta;
     const int* steps;        // [E] n per edge
@@ -116,6 +116,9 @@ struct RecordsParams {
 constexpr int kMaxEnvGroups = 32;
 constexpr int kMaxTableSpheres = 128;
 constexpr int kRecordsWarps = 4;  // warps per CTA of the records check kernel
+// Entries of a warp's (primitive, link) pair list in shared memory; a pair with
+// more candidates is walked in segments of this many.
+constexpr int kPairCap = 1024;
 
 // One robot's pipeline, instantiated in its own translation unit
 // (bcc_robot_<name>.cu) from the templates of bcc_pipeline.cuh.

@@ -17,13 +17,14 @@
 //   5. swept_kernel        per (edge, link) AABB of the link's cull sphere over
 //                          all the edge's samples
 //   6. check_kernel        CTA = one environment x a tile of edges.  The
-//                          environment's blob (primitive records + interval-mask
-//                          cull tables) is staged into shared memory once by a
-//                          cp.async.bulk copy and reused by every edge of the tile.
-//                          Each warp takes one edge at a time: lane g turns link
-//                          g's swept AABB into three slab ranges and ANDs three
-//                          64-bit primitive masks (the cull), the surviving
-//                          (primitive, link) pairs are compacted, and the warp walks
+//                          environment's primitive records are staged into shared
+//                          memory once by a cp.async.bulk copy and reused by every
+//                          edge of the tile.  Each warp takes one edge at a time:
+//                          lane g turns link g's swept AABB into three slab ranges
+//                          and ANDs three 64-bit primitive masks of the
+//                          environment's interval-mask tables (the cull, read
+//                          through L1), the surviving (primitive, link) pairs are
+//                          compacted (lane g writes link g's), and the warp walks
 //                          (sample, pair) items 32 at a time in check order with a
 //                          warp-ballot exit on the first hit.
 //
@@ -407,9 +408,12 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
     const int np = (int)(shape & 0xffffu);
     const int W = (int)(shape >> 16);  // 64-bit words per primitive mask
     const float4* prim = reinterpret_cast<const float4*>(smem);
-    const uint64_t* masks = reinterpret_cast<const uint64_t*>(smem + (size_t)np * kPrimF4 * 16);
-    uint16_t* pairs = reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) +
-                      (size_t)warp * P.pairs_per_warp;
+    // the mask tables stay in global memory (read through L1): each pair reads
+    // only the few words its slab ranges select
+    const uint64_t* __restrict__ masks =
+        reinterpret_cast<const uint64_t*>(P.blobs + (size_t)__float_as_uint(h0.w) + (size_t)np * kPrimF4);
+    const int K = P.pairs_per_warp;
+    uint16_t* pairs = reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) + (size_t)warp * K;
 
     for (int slot = warp; slot < n_slots; slot += WARPS) {
         const int e = MODE == 2 ? P.q_edges[(size_t)cta * P.edges_per_cta + slot] : e_begin + slot;
@@ -429,33 +433,41 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
             tz = slab_tri(lo.z, hi.z, h0.z, h1.z);
         }
         const bool live = tx >= 0 && ty >= 0 && tz >= 0;
-        // Compact the surviving (primitive, link) pairs, link-major: for each link
-        // the whole warp writes that link's mask bits, lane l owning bits l, l + 32.
-        int C = 0;
-        const uint32_t lt = (1u << lane) - 1u;
-        for (int w = 0; w < W; ++w) {
-            uint64_t mine = 0;
-            if (live) {
-                mine = masks[((size_t)0 * kGridTri + tx) * W + w] & masks[((size_t)1 * kGridTri + ty) * W + w] &
-                       masks[((size_t)2 * kGridTri + tz) * W + w];
-            }
-#pragma unroll 1
-            for (int g = 0; g < G; ++g) {
-                const uint32_t mlo = __shfl_sync(kFull, (uint32_t)mine, g);
-                const uint32_t mhi = __shfl_sync(kFull, (uint32_t)(mine >> 32), g);
-                if ((mlo | mhi) == 0u) continue;
-                const int clo = __popc(mlo);
-                if ((mlo >> lane) & 1u) pairs[C + __popc(mlo & lt)] = (uint16_t)(((w * 64 + lane) << GB) | g);
-                if ((mhi >> lane) & 1u)
-                    pairs[C + clo + __popc(mhi & lt)] = (uint16_t)(((w * 64 + 32 + lane) << GB) | g);
-                C += clo + __popc(mhi);
-            }
+        // Compact the surviving (primitive, link) pairs, link-major: lane g counts
+        // link g's candidates, an exclusive warp scan gives each link its offset,
+        // and every lane writes its own link's pairs in primitive order.
+        const int ox = (live ? tx : 0) * W, oy = (kGridTri + (live ? ty : 0)) * W,
+                  oz = (2 * kGridTri + (live ? tz : 0)) * W;
+        int cnt = 0;
+        if (live)
+            for (int w = 0; w < W; ++w) cnt += __popcll(__ldg(masks + ox + w) & __ldg(masks + oy + w) & __ldg(masks + oz + w));
+        int off = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, off, o);
+            if (lane >= o) off += y;
         }
-        __syncwarp();
+        const int C = __shfl_sync(kFull, off, 31);
+        off -= cnt;
 
         bool collide = false, undecided = false;
         WalkStats st;
-        if (C > 0) {
+        // Pairs [seg0, seg0 + K) at a time (one segment unless C > K).
+        for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
+            const int seg1 = min(C, seg0 + K);
+            if (cnt > 0 && off < seg1 && off + cnt > seg0) {
+                int idx = off;
+                for (int w = 0; w < W && idx < seg1; ++w) {
+                    uint64_t m = __ldg(masks + ox + w) & __ldg(masks + oy + w) & __ldg(masks + oz + w);
+                    while (m && idx < seg1) {
+                        const int b = __ffsll((long long)m) - 1;
+                        if (idx >= seg0) pairs[idx - seg0] = (uint16_t)(((w * 64 + b) << GB) | lane);
+                        ++idx;
+                        m &= m - 1;
+                    }
+                }
+            }
+            __syncwarp();
             const int n = P.steps[e];
             const size_t row0 = (size_t)P.offs[e];
             // Learned order: rank the edge's 4 n segments by their MLP score
@@ -478,10 +490,10 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
                 if (lane + 32 < nseg) s_perm[warp][rank1] = (uint8_t)(lane + 32);
                 __syncwarp();
             }
-            collide = walk_pairs<M, MODE>(P.table, row0, n, C, pairs, prim, np, learned ? s_perm[warp] : nullptr,
-                                          P.queue_min_items, undecided, st);
+            collide = walk_pairs<M, MODE>(P.table, row0, n, seg1 - seg0, pairs, prim, np,
+                                          learned ? s_perm[warp] : nullptr, P.queue_min_items, undecided, st);
+            __syncwarp();  // every lane is done with this segment's pairs
         }
-        __syncwarp();
         if (MODE == 1 && undecided) {
             if (lane == 0) {
                 const int n = P.steps[e];
@@ -516,14 +528,17 @@ __device__ __forceinline__ int tile_slots(const CheckParams& P, int env, int til
     return min(P.edges_per_cta, P.num_edges - e_begin);
 }
 
-__device__ __forceinline__ uint32_t blob_bytes_of(float4 h1) {
-    const uint32_t shape = __float_as_uint(h1.w);
-    return (shape & 0xffffu) * kPrimF4 * 16u + 3u * kGridTri * (shape >> 16) * 8u;
+// Bytes of an environment's primitive records (what a CTA stages).
+__device__ __forceinline__ uint32_t record_bytes_of(float4 h1) {
+    return (__float_as_uint(h1.w) & 0xffffu) * kPrimF4 * 16u;
 }
 
 // One CTA per (environment, edge tile): blockIdx.x = environment, blockIdx.y = tile.
+// Check CTAs are sized for 32 resident warps per SM (at most 64 registers).
+constexpr int kCheckWarpsPerSM = 32;
+
 template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
+__global__ void __launch_bounds__(WARPS * 32, kCheckWarpsPerSM / WARPS) check_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ uint8_t s_perm[WARPS][kMaxSegments];
@@ -532,7 +547,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
     if (n_slots <= 0) return;
     const float4 h0 = P.env_hdr[2 * env + 0];
     const float4 h1 = P.env_hdr[2 * env + 1];
-    const uint32_t bytes = blob_bytes_of(h1);
+    const uint32_t bytes = record_bytes_of(h1);
     if (bytes) {
         if (threadIdx.x == 0) {
             mbar_init(&bar, 1);
@@ -555,7 +570,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_kernel(CheckParams P) {
 constexpr int kItemsPerGrab = 2;
 
 template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32) check_persistent_kernel(CheckParams P) {
+__global__ void __launch_bounds__(WARPS * 32, kCheckWarpsPerSM / WARPS) check_persistent_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ uint8_t s_perm[WARPS][kMaxSegments];
@@ -583,7 +598,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_persistent_kernel(CheckParam
             const float4 h0 = P.env_hdr[2 * env + 0];
             const float4 h1 = P.env_hdr[2 * env + 1];
             if (env != staged) {
-                const uint32_t bytes = blob_bytes_of(h1);
+                const uint32_t bytes = record_bytes_of(h1);
                 __syncthreads();  // every warp is done with the previous blob
                 if (bytes) {
                     if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)__float_as_uint(h0.w), bytes, &bar);
@@ -813,7 +828,7 @@ cudaError_t run_steps(const PipelineArgs& a, cudaStream_t st) {
 
 template <class M, int W, int MODE>
 cudaError_t launch_check_wm(CheckParams P, int E, cudaStream_t st) {
-    P.pairs_per_warp = (P.max_prims * M::num_env_groups + 7) & ~7;
+    P.pairs_per_warp = std::min((P.max_prims * M::num_env_groups + 7) & ~7, kPairCap);
     const size_t smem = P.blob_smem + (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
     if (P.persistent) {
         cudaError_t err = cudaFuncSetAttribute(check_persistent_kernel<M, W, MODE>,
