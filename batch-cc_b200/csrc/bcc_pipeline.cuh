@@ -452,9 +452,9 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
 
         bool collide = false, undecided = false;
         WalkStats st;
-        // Pairs [seg0, seg0 + K) at a time (one segment unless C > K).
-        for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
-            const int seg1 = min(C, seg0 + K);
+        // Pair list entries [seg0, seg1): lane g writes link g's candidates that
+        // fall in the range.
+        auto write_seg = [&](int seg0, int seg1) {
             if (cnt > 0 && off < seg1 && off + cnt > seg0) {
                 int idx = off;
                 for (int w = 0; w < W && idx < seg1; ++w) {
@@ -468,6 +468,8 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
                 }
             }
             __syncwarp();
+        };
+        auto walk_seg = [&](int Cs) {
             const int n = P.steps[e];
             const size_t row0 = (size_t)P.offs[e];
             // Learned order: rank the edge's 4 n segments by their MLP score
@@ -490,9 +492,24 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
                 if (lane + 32 < nseg) s_perm[warp][rank1] = (uint8_t)(lane + 32);
                 __syncwarp();
             }
-            collide = walk_pairs<M, MODE>(P.table, row0, n, seg1 - seg0, pairs, prim, np,
+            collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np,
                                           learned ? s_perm[warp] : nullptr, P.queue_min_items, undecided, st);
             __syncwarp();  // every lane is done with this segment's pairs
+        };
+        // Robots whose leaves all lie inside their bounds have a small walk: a
+        // separate copy for the usual single-segment case keeps the segment
+        // bookkeeping out of it.  The overhang-aware walk stays in one copy.
+        bool single = false;
+        if constexpr (!has_overhang<M>()) single = C > 0 && C <= K;
+        if (single) {
+            write_seg(0, C);
+            walk_seg(C);
+        } else {
+            for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
+                const int seg1 = min(C, seg0 + K);
+                write_seg(seg0, seg1);
+                walk_seg(seg1 - seg0);
+            }
         }
         if (MODE == 1 && undecided) {
             if (lane == 0) {
