@@ -282,8 +282,12 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
     const DevTables<M>& T = tab<M>();
     const int lane = threadIdx.x & 31;
     const int total = kLanes * n * C;
-    const int dr = 32 / C, dc = 32 % C;
-    int r = lane / C, c = lane - (lane / C) * C;
+    // a / C for a <= 32 and 1 <= C <= kPairCap: floor((a + 0.5) / C) in FP32 is
+    // exact (the quotient stays >= 1 / 2048 away from an integer), and cheaper
+    // than an integer division by a runtime divisor.
+    const float inv_c = __frcp_rn((float)C);
+    const int dr = (int)(32.5f * inv_c), dc = 32 - dr * C;
+    int r = (int)(((float)lane + 0.5f) * inv_c), c = lane - r * C;
     bool collide = false;
     for (int w0 = 0; w0 < total; w0 += 32) {
         bool gate = false;
