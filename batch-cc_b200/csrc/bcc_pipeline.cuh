@@ -178,25 +178,59 @@ __device__ __forceinline__ bool self_hit(float4 a, float4 b) {
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) - rs * rs < 0.0f;
 }
 
+// One warp per sample row, rows strided over the grid.  Lanes test the self
+// groups' bound pairs 32 at a time; the leaf pairs of every group whose bound
+// pair hit are then tested 32 at a time (the reference's gate-then-leaves,
+// any hit = self-collision).  Rows of an edge already known to self-collide
+// are skipped.  The self tables are staged in shared memory: lanes read
+// different entries, which constant memory would serialise.
+constexpr int kSelfThreads = 256;
+
 template <class M>
-__global__ void __launch_bounds__(128) self_kernel(const float4* __restrict__ table, int total,
-                                                   const int* __restrict__ row_edge,
-                                                   int* __restrict__ edge_self) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= total) return;
-    const float4* sp = table + (size_t)row * M::num_spheres;
+__global__ void __launch_bounds__(kSelfThreads) self_kernel(const float4* __restrict__ table, int total,
+                                                             const int* __restrict__ row_edge,
+                                                             int* __restrict__ edge_self) {
+    constexpr int NG = M::num_self_groups;
+    constexpr int NP = M::num_self_pairs;
+    __shared__ short s_bound[NG][2];
+    __shared__ short s_begin[NG + 1];
+    __shared__ unsigned char s_pairs[NP][2];
     const DevTables<M>& T = tab<M>();
-    bool hit = false;
-    for (int g = 0; g < M::num_self_groups && !hit; ++g) {
-        if (!self_hit(sp[T.self_bound[g][0]], sp[T.self_bound[g][1]])) continue;
-        for (int k = T.self_pair_begin[g]; k < T.self_pair_begin[g + 1]; ++k) {
-            if (self_hit(sp[T.self_pairs[k][0]], sp[T.self_pairs[k][1]])) {
-                hit = true;
-                break;
+    for (int i = threadIdx.x; i < NG; i += blockDim.x) {
+        s_bound[i][0] = (short)T.self_bound[i][0];
+        s_bound[i][1] = (short)T.self_bound[i][1];
+    }
+    for (int i = threadIdx.x; i <= NG; i += blockDim.x) s_begin[i] = (short)T.self_pair_begin[i];
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+        s_pairs[i][0] = T.self_pairs[i][0];
+        s_pairs[i][1] = T.self_pairs[i][1];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < total; row += warps) {
+        const int e = row_edge[row];
+        int decided = lane == 0 ? *(volatile const int*)(edge_self + e) : 0;
+        if (__shfl_sync(kFull, decided, 0)) continue;  // another row already found a self-collision
+        const float4* sp = table + (size_t)row * M::num_spheres;
+        bool hit = false;
+        for (int g0 = 0; g0 < NG && !hit; g0 += 32) {
+            const int g = g0 + lane;
+            const bool gate = g < NG && self_hit(sp[s_bound[g][0]], sp[s_bound[g][1]]);
+            uint32_t gm = __ballot_sync(kFull, gate);
+            while (gm && !hit) {
+                const int gg = g0 + __ffs(gm) - 1;
+                gm &= gm - 1u;
+                const int end = s_begin[gg + 1];
+                for (int k0 = s_begin[gg]; k0 < end && !hit; k0 += 32) {  // warp-uniform trip count
+                    const int k = k0 + lane;
+                    const bool h = k < end && self_hit(sp[s_pairs[k][0]], sp[s_pairs[k][1]]);
+                    hit = __any_sync(kFull, h);
+                }
             }
         }
+        if (hit && lane == 0) atomicOr(edge_self + e, 1);
     }
-    if (hit) atomicOr(edge_self + row_edge[row], 1);
 }
 
 // ------------------------------------------------------------------ 5. swept
@@ -908,7 +942,15 @@ cudaError_t run_prep(const PipelineArgs& a, cudaStream_t st) {
     if (ev) cudaEventRecord(ev[2], st);
     cudaError_t err = cudaMemsetAsync(a.edge_self, 0, sizeof(int) * E, st);
     if (err != cudaSuccess) return err;
-    if (R > 0) self_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
+    if (R > 0) {
+        // one warp per row; a grid of at most 16 CTAs per SM strides over the rows
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long long want = ((long long)R * 32 + kSelfThreads - 1) / kSelfThreads;
+        const int grid = (int)std::min<long long>(want, 16ll * std::max(sms, 1));
+        self_kernel<M><<<grid, kSelfThreads, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
+    }
     if (ev) cudaEventRecord(ev[3], st);
     swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept);
     if (ev) cudaEventRecord(ev[4], st);
