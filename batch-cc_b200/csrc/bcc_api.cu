@@ -178,7 +178,8 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     if (total < 0 || total > (1 << 27))
         return fail(ctx, BCC_ERR_LIMIT, "too many samples in one call (edges too long or non-finite)");
     const int NS = ops->num_spheres;
-    BCC_CUDA(ctx, ctx->table.ensure(sizeof(float4) * (size_t)NS * std::max(total, 1)));
+    const size_t tiles = ((size_t)std::max(total, 1) + bcc::kMaxTableTile - 1) / bcc::kMaxTableTile;
+    BCC_CUDA(ctx, ctx->table.ensure(sizeof(float4) * (size_t)NS * tiles * bcc::kMaxTableTile));
     BCC_CUDA(ctx, ctx->row_edge.ensure(sizeof(int) * (size_t)std::max(total, 1)));
     a.total_rows = total;
     a.table = ctx->table.as<float4>();

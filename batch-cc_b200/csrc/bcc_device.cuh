@@ -132,12 +132,26 @@ __device__ __forceinline__ float4 fk_sphere(const Frames<M, T>& F) {
     return c;
 }
 
-// Write every sphere attached to frame FR into its sample-table position.
+// Sample table layout: rows in tiles of M::table_tile rows, sphere-major inside
+// a tile (a tile of 1 is plain row-major).  With tiles of 32, 32 consecutive
+// rows of one sphere are 512 contiguous bytes and the FK kernel's warp (32
+// consecutive rows) writes each sphere with one coalesced store; row-major keeps
+// a row's bounds and leaves together for the check kernel's reads.
+constexpr int kMaxTableTile = 32;  // hosts round row counts up to this
+
+template <class M>
+__host__ __device__ __forceinline__ size_t table_index(size_t row, int s) {
+    constexpr int TT = M::table_tile;
+    return ((row / TT) * M::num_spheres + s) * TT + (row % TT);
+}
+
+// Write every sphere attached to frame FR into its sample-table position; `out`
+// points at the row's first sphere, spheres M::table_tile float4 apart.
 template <class M, int FR, int S, class T>
 __device__ __forceinline__ void emit_one(const Frames<M, T>& F, float4* __restrict__ out) {
     if constexpr (M::sphere_frame[S] == FR) {
         constexpr int pos = M::table_pos[S];
-        out[pos] = fk_sphere<M, S, T>(F);
+        out[pos * M::table_tile] = fk_sphere<M, S, T>(F);
     }
 }
 template <class M, int FR, class T, int... S>
@@ -198,7 +212,7 @@ struct FkJoint<M, M::dof, T> {
     __device__ __forceinline__ static void run(const float*, Frames<M, T>&, float4* __restrict__) {}
 };
 
-// All sphere centres of configuration q into out[table_pos[s]].
+// All sphere centres of configuration q into out[table_pos[s] * table_tile].
 template <class M>
 __device__ __forceinline__ void fk_spheres(const float* q, float4* __restrict__ out) {
     using T = typename std::conditional<M::fk_precision == 64, double, float>::type;

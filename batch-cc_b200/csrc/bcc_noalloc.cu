@@ -39,6 +39,7 @@ static __device__ __align__(256) int g_steps[kMaxEdges];
 static __device__ __align__(256) int g_offs[kMaxEdges + 1];
 static __device__ __align__(256) int g_edge_self[kMaxEdges];
 static __device__ __align__(256) float4 g_swept[kMaxEdges * kGroupsMax * 2];
+static_assert(kMaxRows % bcc::kMaxTableTile == 0, "the sample table holds whole tiles of rows");
 static __device__ __align__(256) float4 g_table[kMaxRows * kNumSpheresMax];
 static __device__ __align__(256) int g_row_edge[kMaxRows];
 static __device__ __align__(256) int g_error[1];

@@ -77,6 +77,7 @@ DevTables<M> host_tables() {
     static_assert(M::num_env_groups <= kMaxEnvGroups, "one cull lane per link group");
     static_assert(M::num_spheres <= kMaxTableSpheres, "sample-table row width");
     static_assert(M::num_spheres <= 256, "self pairs hold 8-bit row positions");
+    static_assert(M::table_tile >= 1 && kMaxTableTile % M::table_tile == 0, "table tiles divide the row padding");
     DevTables<M> t;
     for (int g = 0; g < M::num_env_groups; ++g) {
         t.env_bound[g] = M::env_bound[g];
@@ -142,7 +143,8 @@ __global__ void edge_steps_kernel(const float* __restrict__ edges, int E, int re
 // ------------------------------------------------------------------ 3. FK
 // Sample table row: num_spheres float4 (centre xyz, radius) in table_pos order
 // (env-group bounds, then env leaves, then the rest), one row per (edge,
-// sample) in edge order then sample index order.
+// sample) in edge order then sample index order; stored in tiles of
+// M::table_tile rows (table_index).
 template <class M>
 __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges, int E,
                                                  const int* __restrict__ steps,
@@ -167,7 +169,7 @@ __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges
         t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
     }
     edge_sample<M::dof>(s, t, steps[e], k, q);
-    fk_spheres<M>(q, table + (size_t)row * M::num_spheres);
+    fk_spheres<M>(q, table + table_index<M>(row, 0));
     row_edge[row] = e;
 }
 
@@ -212,11 +214,11 @@ __global__ void __launch_bounds__(kSelfThreads) self_kernel(const float4* __rest
         const int e = row_edge[row];
         int decided = lane == 0 ? *(volatile const int*)(edge_self + e) : 0;
         if (__shfl_sync(kFull, decided, 0)) continue;  // another row already found a self-collision
-        const float4* sp = table + (size_t)row * M::num_spheres;
+        const float4* sp = table + table_index<M>(row, 0);  // sphere s at sp[s * M::table_tile]
         bool hit = false;
         for (int g0 = 0; g0 < NG && !hit; g0 += 32) {
             const int g = g0 + lane;
-            const bool gate = g < NG && self_hit(sp[s_bound[g][0]], sp[s_bound[g][1]]);
+            const bool gate = g < NG && self_hit(sp[s_bound[g][0] * M::table_tile], sp[s_bound[g][1] * M::table_tile]);
             uint32_t gm = __ballot_sync(kFull, gate);
             while (gm && !hit) {
                 const int gg = g0 + __ffs(gm) - 1;
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(kSelfThreads) self_kernel(const float4* __rest
                 const int end = s_begin[gg + 1];
                 for (int k0 = s_begin[gg]; k0 < end && !hit; k0 += 32) {  // warp-uniform trip count
                     const int k = k0 + lane;
-                    const bool h = k < end && self_hit(sp[s_pairs[k][0]], sp[s_pairs[k][1]]);
+                    const bool h = k < end && self_hit(sp[s_pairs[k][0] * M::table_tile], sp[s_pairs[k][1] * M::table_tile]);
                     hit = __any_sync(kFull, h);
                 }
             }
@@ -249,7 +251,7 @@ __global__ void swept_kernel(const float4* __restrict__ table, const int* __rest
         const int b = g;  // bounds lead every table row
         float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int r = r0 + lane; r < r1; r += 32) {
-            const float4 c = table[(size_t)r * M::num_spheres + b];
+            const float4 c = table[table_index<M>(r, b)];
             lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
             hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
         }
@@ -288,7 +290,7 @@ template <class M>
 __device__ __forceinline__ bool bound_hits_any(const float4* __restrict__ table, size_t row0, int k, int g,
                                                const float4* prim, int np) {
     const int lane = threadIdx.x & 31;
-    float4 b = table[(row0 + (size_t)k) * M::num_spheres + g];
+    float4 b = table[table_index<M>(row0 + (size_t)k, g)];
     b.w += kEnvInflate;
     bool any = false;
     for (int p = lane; p < np; p += 32) any |= sphere_hits_prim(b, prim + p * kPrimF4);
@@ -331,7 +333,7 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
             const uint32_t pr = pairs[c];
             g = (int)(pr & ((1u << GB) - 1u));
             p = (int)(pr >> GB);
-            float4 bs = table[(row0 + (size_t)k) * M::num_spheres + g];
+            float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
             bs.w += kEnvInflate;
             float rho;
             const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
@@ -374,7 +376,7 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 bool hit = false;
                 if (t < L) {
                     const int leaf = j_first + (t - (j_incl - j_cnt));
-                    float4 ls = table[(row0 + (size_t)j_k) * M::num_spheres + G + leaf];
+                    float4 ls = table[table_index<M>(row0 + (size_t)j_k, G + leaf)];
                     ls.w += kEnvInflate;
                     hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
                 }
@@ -761,17 +763,17 @@ __global__ void training_rows_kernel(CheckParams P, const float* __restrict__ ed
     const float4 hd0 = P.env_hdr[2 * env], hd1 = P.env_hdr[2 * env + 1];
     const float4* rec = P.blobs + __float_as_uint(hd0.w);
     const int np = (int)(__float_as_uint(hd1.w) & 0xffffu);
-    const float4* row = P.table + ((size_t)P.offs[e] + k) * M::num_spheres;
+    const float4* row = P.table + table_index<M>((size_t)P.offs[e] + k, 0);  // stride M::table_tile
     const DevTables<M>& T = tab<M>();
     bool hit = false;
     for (int g = 0; g < G && !hit; ++g) {
-        float4 b = row[g];
+        float4 b = row[g * M::table_tile];
         b.w += kEnvInflate;
         bool gate = false;
         for (int p = 0; p < np && !gate; ++p) gate = sphere_hits_prim(b, rec + p * kPrimF4);
         if (!gate) continue;
         for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1] && !hit; ++li) {
-            float4 l = row[G + li];
+            float4 l = row[(G + li) * M::table_tile];
             l.w += kEnvInflate;
             for (int p = 0; p < np && !hit; ++p) hit = sphere_hits_prim(l, rec + p * kPrimF4);
         }

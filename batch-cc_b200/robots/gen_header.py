@@ -33,6 +33,13 @@ LIMITS = {
 # algorithmic FLOP count.
 FK_FLOPS = {"panda": 1150, "fetch": 983, "baxter": 1792}
 
+# Rows per tile of the sample table (sphere-major inside a tile): 32 makes the FK
+# kernel's stores coalesced, 1 keeps each row contiguous for the check kernel's
+# bound and leaf reads.  Measured on B200: tiling speeds up the Fetch and Baxter
+# checks (126 / 107 spheres per row, FP64 FK) by 5-6 % and slows Panda's (70
+# spheres, a check dominated by its walk) by 6 %.
+TABLE_TILE = {"panda": 1, "fetch": 32, "baxter": 32}
+
 
 def rpy_matrix(r, p, y):
     cr, sr = math.cos(r), math.sin(r)
@@ -80,6 +87,8 @@ def main():
     w("    // (32: float expressions; 64: double expressions, centres rounded to float).")
     w("    static constexpr int fk_precision = %d;" % m.get("fk_precision", 32))
     w("    static constexpr int fk_flops = %d;" % FK_FLOPS[name])
+    w("    // Sample-table rows per tile (sphere-major inside a tile; 1 = row-major).")
+    w("    static constexpr int table_tile = %d;" % TABLE_TILE[name])
     w("")
     w("    // Fixed transform of joint k (row-major 3x4: rotation | translation).")
     w("    // frame k+1 = frame joint_parent[k] * F_k * J_k(q_k), J = Rz(q) for a revolute")
