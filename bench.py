@@ -33,6 +33,17 @@ UNIT = "edges/s"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
+def committed_traffic(workload_name_):
+    """DRAM bytes of one check_kernel launch on a full-size workload, from the
+    committed ncu summary (None when the workload has no capture)."""
+    import re
+    path = os.path.join(ROOT, "profiles", "check_kernel_dram_traffic.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"^traffic_bytes %s (\d+)$" % re.escape(workload_name_), open(path).read(), re.M)
+    return int(m.group(1)) if m else None
+
+
 def metric_of(name, N):
     """The headline metric on the headline workload; the same quantity, named
     for its robot and size, on the others."""
@@ -440,8 +451,12 @@ def run_ours(args, world, rank, local, dist):
     flops, rel_err = algorithmic_flops(envs, edges, args.flop_sample, robot)
     chk_ms = statistics.mean(results["plain"][1])
     achieved = flops / (chk_ms * 1e-3) / 1e12
+    traffic = committed_traffic(args.workload) if (args.envs is None and args.edges is None) else None
     line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "traffic": None,
+                        "frac": achieved / peak, "traffic": traffic,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one check_kernel "
+                                          "launch on this workload (profiles/check_kernel_dram_traffic.md)"
+                        if traffic else None,
                         "kernel": "check_kernel (plain order)", "kernel_ms": chk_ms,
                         "algorithmic_flops_per_launch": flops, "flop_estimate_rel_stderr": rel_err,
                         "peak_source": "FP32 FMA probe kernel measured in this run (bcc_measure_fp32_peak); "
