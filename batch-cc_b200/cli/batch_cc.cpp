@@ -1,12 +1,15 @@
-// batch_cc -- command-line driver, drop-in for the reference driver
-// (scripts/batch_cc_mbm.cpp:181-207):
+// batch_cc -- command-line driver, drop-in for the reference drivers:
 //
 //     batch_cc <robot_name> <num_environments> <num_edges> [problems.json | scene.txt]
+//         (scripts/batch_cc_mbm.cpp:181-207) environments from the
+//         MotionBenchMaker problem file scripts/<robot>_problems.json (or the
+//         given file; a .txt file is read as a scene file); edges are
+//         consecutive Halton samples scaled into the joint limits;
+//     batch_cc <robot_name> <graph.dot> <scene.txt>
+//         (scripts/batch_cc.cpp:331-425) the edges of a roadmap graph whose
+//         vertices carry `states`, checked in all 200 scene environments.
 //
-// Environments come from the MotionBenchMaker problem file
-// scripts/<robot>_problems.json (or the given file; a .txt file is read as a
-// scene file); edges are consecutive Halton samples scaled into the joint
-// limits; resolution 32.  Prints the checker's timing lines and one line
+// Resolution 32.  Prints the checker's timing lines and one line
 // "Edge i: v v v ..." per edge (v = 1 when the edge collides in environment j).
 #include <cstdio>
 #include <cstdlib>
@@ -14,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "dot.hh"
 #include "loaders.hh"
 #include "src/Robots.hh"
 #include "src/batch_cc.hh"
@@ -83,9 +87,64 @@ int run(int num_envs, int num_edges, const std::string& path) {
     return 0;
 }
 
+// Environments a scene file defines (MAX_WORLD_SAMPLES_EVAL, scripts/batch_cc.cpp:25).
+constexpr int kSceneEnvs = 200;
+
+template <typename Robot>
+int run_graph(const std::string& graph_path, const std::string& scene_path) {
+    std::vector<ppln::collision::Environment<float>> envs = bcc_loaders::load_scene(scene_path, kSceneEnvs);
+    const bcc_dot::Graph g = bcc_dot::parse(bcc_loaders::read_file(graph_path));
+    std::vector<std::array<typename Robot::Configuration, 2>> edges;
+    edges.reserve(g.edges.size());
+    for (const auto& e : g.edges) {
+        const auto& a = g.states[e.first];
+        const auto& b = g.states[e.second];
+        if ((int)a.size() < Robot::dimension || (int)b.size() < Robot::dimension)
+            throw std::runtime_error("graph vertex with fewer states than the robot's joints");
+        std::array<typename Robot::Configuration, 2> edge;
+        for (int i = 0; i < Robot::dimension; ++i) {
+            edge[0][i] = (float)a[i];
+            edge[1][i] = (float)b[i];
+        }
+        edges.push_back(edge);
+    }
+    std::cout << "Number of edges: " << edges.size() << "\n";
+    std::cout << "Number of environments: " << envs.size() << "\n";
+    if (const char* dump = std::getenv("BCC_DUMP_INPUTS")) dump_inputs<Robot>(dump, envs, edges);
+    std::vector<bool> results(edges.size() * envs.size());
+    batch_cc::batch_cc<Robot>(envs, edges, 32, results);
+    for (size_t i = 0; i < edges.size(); ++i) {
+        std::cout << "Edge " << i << ": ";
+        for (size_t j = 0; j < envs.size(); ++j) std::cout << results[i * envs.size() + j] << " ";
+        std::cout << "\n";
+    }
+    for (size_t i = 0; i < envs.size(); ++i)
+        std::cout << "Environment " << i << ": " << envs[i].num_spheres << " spheres, " << envs[i].num_cuboids
+                  << " cuboids, " << envs[i].num_capsules << " capsules\n\n";
+    return 0;
+}
+
+inline bool ends_with(const std::string& s, const std::string& t) {
+    return s.size() >= t.size() && s.compare(s.size() - t.size(), t.size(), t) == 0;
+}
+
 int main(int argc, char** argv) {
+    if (argc == 4 && ends_with(argv[2], ".dot")) {  // roadmap graph mode
+        const std::string robot = argv[1];
+        try {
+            if (robot == "panda") return run_graph<ppln::robots::Panda>(argv[2], argv[3]);
+            if (robot == "fetch") return run_graph<ppln::robots::Fetch>(argv[2], argv[3]);
+            if (robot == "baxter") return run_graph<ppln::robots::Baxter>(argv[2], argv[3]);
+        } catch (const std::exception& e) {
+            std::cerr << "batch_cc: " << e.what() << "\n";
+            return 2;
+        }
+        std::cout << "Unknown robot name: " << robot << "\n";
+        return -1;
+    }
     if (argc != 4 && argc != 5) {
-        std::cout << "Usage: ./batch_cc <robot_name> <num_environments> <num_edges>\n";
+        std::cout << "Usage: ./batch_cc <robot_name> <num_environments> <num_edges>\n"
+                     "       ./batch_cc <robot_name> <graph.dot> <scene.txt>\n";
         return 1;
     }
     const std::string robot = argv[1];

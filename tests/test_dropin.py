@@ -91,3 +91,49 @@ def test_cli_usage_and_unknown_robot():
     assert r.returncode == 1 and r.stdout.startswith("Usage:")
     r = subprocess.run([CLI, "xarm7", "1", "1", os.devnull], capture_output=True, text=True)
     assert r.returncode == 255 and "Unknown robot name" in r.stdout
+
+
+def _roadmap():
+    """Vertices and edges of tests/golden/roadmap_small.dot, read with regexes."""
+    import re
+    text = open(os.path.join(ROOT, "tests", "golden", "roadmap_small.dot")).read()
+    states = {int(m.group(1)): [float(v) for v in m.group(2).split()]
+              for m in re.finditer(r'^(\d+)\[states="([^"]*)"\];$', text, re.M)}
+    edges = []
+    for line in text.splitlines():
+        if "--" in line:
+            ids = [int(t) for t in re.findall(r"\d+(?=\s*(?:--|;|\[))", line.split("[")[0] + ";")]
+            edges += list(zip(ids[:-1], ids[1:]))
+    return states, edges
+
+
+def test_cli_graph_mode_reads_the_roadmap(tmp_path):
+    """`batch_cc <robot> <graph.dot> <scene.txt>`: edges in file order with their
+    vertices' states (chains included), 200 scene environments -- checked on the
+    inputs the driver dumps before it checks (without a GPU the check then fails)."""
+    import numpy as np
+    dump = str(tmp_path / "inputs.bin")
+    env = dict(os.environ, BCC_DUMP_INPUTS=dump)
+    r = subprocess.run([CLI, "panda", "tests/golden/roadmap_small.dot", "tests/golden/scene_small.txt"],
+                       capture_output=True, text=True, env=env, cwd=ROOT, timeout=120)
+    states, edges = _roadmap()
+    assert "Number of edges: %d" % len(edges) in r.stdout
+    assert "Number of environments: 200" in r.stdout
+    raw = open(dump, "rb").read()
+    N, E, dof = np.frombuffer(raw[:12], np.int32)
+    assert (N, E, dof) == (200, len(edges), 7)
+    got = np.frombuffer(raw[-4 * E * 2 * dof:], np.float32).reshape(E, 2, dof)
+    want = np.array([[states[a], states[b]] for a, b in edges], np.float32)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("text,msg", [("digraph G { a -> b }", "fewer states"),
+                                      ("graph G { subgraph s { a } }", "subgraphs"),
+                                      ("graph G { a [states=\"1 2\"", "unterminated"),
+                                      ("tree G { }", "expected graph")])
+def test_cli_graph_mode_rejects_bad_files(tmp_path, text, msg):
+    p = tmp_path / "g.dot"
+    p.write_text(text)
+    r = subprocess.run([CLI, "panda", str(p), "tests/golden/scene_small.txt"], capture_output=True, text=True,
+                       cwd=ROOT, timeout=60)
+    assert r.returncode == 2 and msg in r.stderr, (r.returncode, r.stderr)

@@ -1,7 +1,8 @@
 """GPU test of the drop-in CLI driver (batch_cc <robot> <num_envs> <num_edges>
-[file]) through the C++ facade: its printed verdicts equal the oracle's and
-the reference CUDA path's on the exact inputs it checked (dumped by the
-driver), for problem-file and scene-file environments."""
+[file], and batch_cc <robot> <graph.dot> <scene.txt>) through the C++ facade:
+its printed verdicts equal the oracle's and the reference CUDA path's on the
+exact inputs it checked (dumped by the driver), for problem-file and scene-file
+environments and roadmap-graph edges."""
 import os
 import subprocess
 
@@ -48,10 +49,13 @@ def run_cli(tmp_path, args):
 
 
 @pytest.mark.parametrize("args", [["panda", "21", "64", "tests/golden/panda_problems_small.json"],
-                                  ["panda", "8", "96", "tests/golden/scene_small.txt"]])
+                                  ["panda", "8", "96", "tests/golden/scene_small.txt"],
+                                  ["panda", "tests/golden/roadmap_small.dot", "tests/golden/scene_small.txt"]])
 def test_cli_matches_oracle_and_reference(tmp_path, args):
     got, envs, edges = run_cli(tmp_path, args)
-    assert got.shape == (int(args[2]), envs.num_envs)
+    assert got.shape == (len(edges), envs.num_envs)
+    if not args[1].endswith(".dot"):
+        assert got.shape[0] == int(args[2])
     n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, orc.check(envs, edges))
     assert len(bad) == 0
     if ref.available():
