@@ -301,6 +301,24 @@ struct WalkStats {
     unsigned long long chunks = 0, gates = 0, leaf = 0;
 };
 
+// Lane g's copy of link group g's leaf range.  The walk can fetch a group's
+// entries with one shuffle per field: its lanes hold items of different groups,
+// and indexing __constant__ memory with a lane-dependent group serialises the
+// access once per distinct group.
+struct GroupLanes {
+    int first, cnt;
+};
+
+template <class M>
+__device__ __forceinline__ GroupLanes group_lanes() {
+    const DevTables<M>& T = tab<M>();
+    const int g = min(threadIdx.x & 31, M::num_env_groups - 1);
+    GroupLanes r;
+    r.first = T.leaf_begin[g];
+    r.cnt = T.leaf_begin[g + 1] - r.first;
+    return r;
+}
+
 // Whole warp: walk (sample rank, pair) items 32 at a time in check order --
 // plain reference order, or with `perm` the edge's segments in learned order --
 // and return whether some item collides.  MODE 1 (probe) stops after the
@@ -311,11 +329,11 @@ struct WalkStats {
 template <class M, int MODE>
 __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, size_t row0, int n, int C,
                                            const uint16_t* pairs, const float4* prim, int np, const uint8_t* perm,
-                                           int queue_min_items, bool& undecided, WalkStats& st) {
+                                           int queue_min_items, const GroupLanes& GL, bool& undecided,
+                                           WalkStats& st) {
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
     constexpr bool kOver = has_overhang<M>();
-    const DevTables<M>& T = tab<M>();
     const int lane = threadIdx.x & 31;
     const int total = kLanes * n * C;
     // a / C for a <= 32 and 1 <= C <= kPairCap: floor((a + 0.5) / C) in FP32 is
@@ -327,26 +345,48 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
     bool collide = false;
     for (int w0 = 0; w0 < total; w0 += 32) {
         bool gate = false;
-        int g = 0, p = 0, k = 0, cnt = 0;
-        if (w0 + lane < total) {
-            k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+        int g = 0, p = 0, k = 0, cnt = 0, first = 0;
+        if constexpr (!kOver) {
+            // c < C on every lane, also past the last item: the pair is decoded and
+            // its group's leaf range fetched by shuffle on every lane (measured
+            // faster for Panda than lane-indexed constant memory), the table and
+            // the primitive read only for live items.
             const uint32_t pr = pairs[c];
             g = (int)(pr & ((1u << GB) - 1u));
             p = (int)(pr >> GB);
-            float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
-            bs.w += kEnvInflate;
-            float rho;
-            const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
-            const float rr = bs.w + rho;
-            gate = d2 - rr * rr < 0.0f;
-            cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
-            if constexpr (kOver) {
+            first = __shfl_sync(kFull, GL.first, g);
+            const int gcnt = __shfl_sync(kFull, GL.cnt, g);
+            if (w0 + lane < total) {
+                k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+                float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
+                bs.w += kEnvInflate;
+                gate = sphere_hits_prim(bs, prim + p * kPrimF4);
+                cnt = gate ? gcnt : 0;
+            }
+        } else {
+            // The overhang-aware walk reads its group fields from constant memory,
+            // which leaves its longer body the registers it needs (measured faster
+            // for Fetch and Baxter).
+            const DevTables<M>& T = tab<M>();
+            if (w0 + lane < total) {
+                k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+                const uint32_t pr = pairs[c];
+                g = (int)(pr & ((1u << GB) - 1u));
+                p = (int)(pr >> GB);
+                float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
+                bs.w += kEnvInflate;
+                float rho;
+                const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
+                const float rr = bs.w + rho;
+                gate = d2 - rr * rr < 0.0f;
+                cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
                 // overhanging leaves (listed first) near a primitive the bound misses
                 if (!gate && T.over_count[g] > 0) {
                     const float rp = rr + T.cull_pad[g];
                     if (d2 - rp * rp < 0.0f) cnt = T.over_count[g];
                 }
             }
+            first = T.leaf_begin[g];
         }
         ++st.chunks;
         if (__any_sync(kFull, cnt > 0)) {
@@ -358,7 +398,6 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 if (lane >= o) incl += y;
             }
             const int L = __shfl_sync(kFull, incl, 31);
-            const int first = T.leaf_begin[g];
             for (int t0 = 0; t0 < L; t0 += 32) {
                 const int t = t0 + lane;
                 // owner j: the first lane whose inclusive count exceeds t
@@ -454,6 +493,7 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
         reinterpret_cast<const uint64_t*>(P.blobs + (size_t)__float_as_uint(h0.w) + (size_t)np * kPrimF4);
     const int K = P.pairs_per_warp;
     uint16_t* pairs = reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) + (size_t)warp * K;
+    const GroupLanes GL = group_lanes<M>();
 
     for (int slot = warp; slot < n_slots; slot += WARPS) {
         const int e = MODE == 2 ? P.q_edges[(size_t)cta * P.edges_per_cta + slot] : e_begin + slot;
@@ -533,7 +573,7 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
                 __syncwarp();
             }
             collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np,
-                                          learned ? s_perm[warp] : nullptr, P.queue_min_items, undecided, st);
+                                          learned ? s_perm[warp] : nullptr, P.queue_min_items, GL, undecided, st);
             __syncwarp();  // every lane is done with this segment's pairs
         };
         // Robots whose leaves all lie inside their bounds have a small walk: a
@@ -823,6 +863,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_records_kernel(RecordsParams
         }
     }
     const uint32_t lt = (1u << lane) - 1u;
+    const GroupLanes GL = group_lanes<M>();
 
     for (int e = e_begin + warp; e < e_end; e += WARPS) {
         uint8_t* out = P.results + (size_t)e * P.num_envs + env;
@@ -866,7 +907,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_records_kernel(RecordsParams
         WalkStats st;
         if (C > 0)
             collide = walk_pairs<M, 0>(P.table, (size_t)P.offs[e], P.steps[e], C, pairs, prim, np, nullptr, 0,
-                                       undecided, st);
+                                       GL, undecided, st);
         __syncwarp();
         if (lane == 0) *out = collide ? 1 : 0;
     }
