@@ -36,19 +36,23 @@ constexpr int kOffW4 = kOffB3 + kMlpHidden;
 constexpr int kOffB4 = kOffW4 + kMlpHidden;
 static_assert(kOffB4 + 1 == kMlpParams, "parameter layout");
 
-// Shared-memory map of the forward kernel (bytes).
+// Shared-memory map of the forward kernel (bytes): the weight images, then per
+// row group its X tile (128 x 48) and H tile (128 x 128), the bias vectors, the
+// groups' mbarriers and the TMEM address slot.
 constexpr uint32_t kImgW1 = kMlpHidden * kMlpIn * 2;       // 12288
 constexpr uint32_t kImgW = kMlpHidden * kMlpHidden * 2;    // 32768
 constexpr uint32_t kSmW1 = 0;
 constexpr uint32_t kSmW2 = kSmW1 + kImgW1;
 constexpr uint32_t kSmW3 = kSmW2 + kImgW;
-constexpr uint32_t kSmX = kSmW3 + kImgW;                   // X tile 128 x 48
-constexpr uint32_t kSmH = kSmX + kImgW1;                   // H tile 128 x 128
-constexpr uint32_t kSmVec = kSmH + kImgW;                  // b1 b2 b3 w4 (4 x 128 floats) + b4
+constexpr int kFwdGroups = 2;                              // independent 128-row tile streams per CTA
+constexpr uint32_t kSmGroup0 = kSmW3 + kImgW;              // group g: X at +g*stride, H at +kImgW1
+constexpr uint32_t kSmGroupStride = kImgW1 + kImgW;
+constexpr uint32_t kSmVec = kSmGroup0 + kFwdGroups * kSmGroupStride;  // b1 b2 b3 w4 (4 x 128) + b4
 constexpr uint32_t kSmBar = kSmVec + 4 * kMlpHidden * 4 + 16;
-constexpr uint32_t kSmTmem = kSmBar + 8;
+constexpr uint32_t kSmTmem = kSmBar + 8 * kFwdGroups;
 constexpr uint32_t kFwdSmem = kSmTmem + 8;
 constexpr uint32_t kImagesBytes = kImgW1 + 2 * kImgW;       // W1T | W2T | W3T
+static_assert(kSmGroup0 % 16 == 0 && kSmGroupStride % 16 == 0, "core-matrix images are 16-byte aligned");
 
 // ---------------------------------------------------------------- images
 // FP32 masters -> BF16 core-matrix images of W1^T [128][48], W2^T, W3^T.
@@ -72,40 +76,70 @@ __global__ void mlp_pack_kernel(const float* __restrict__ params, uint8_t* __res
 // ---------------------------------------------------------------- forward
 // Bias + ReLU of one 128-column accumulator row (this thread's row), written as
 // BF16 into the H image; `taddr` = TMEM address of column 0 of this warp's lanes.
+// One warp group's epilogue of a hidden layer: TMEM accumulator row + bias, ReLU,
+// BF16 into the H image.  Two 16-column loads are in flight before each wait.
 __device__ __forceinline__ void epilogue_relu_to_smem(uint32_t taddr, const float* bias, uint8_t* himg, int row) {
 #pragma unroll 1
-    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
-        float v[16];
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
+        float v[32];
         tc::tmem_ld16(taddr + c0, v);
+        tc::tmem_ld16(taddr + c0 + 16, v + 16);
         tc::wait_ld();
-        uint32_t packed[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float a = fmaxf(v[2 * i] + bias[c0 + 2 * i], 0.0f);
-            const float b = fmaxf(v[2 * i + 1] + bias[c0 + 2 * i + 1], 0.0f);
-            __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-            packed[i] = *reinterpret_cast<uint32_t*>(&h);
+        for (int h = 0; h < 2; ++h) {
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float a = fmaxf(v[16 * h + 2 * i] + bias[c0 + 16 * h + 2 * i], 0.0f);
+                const float b = fmaxf(v[16 * h + 2 * i + 1] + bias[c0 + 16 * h + 2 * i + 1], 0.0f);
+                __nv_bfloat162 hh = __floats2bfloat162_rn(a, b);
+                packed[i] = *reinterpret_cast<uint32_t*>(&hh);
+            }
+            *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0 + 16 * h, kMlpHidden)) =
+                make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0 + 16 * h + 8, kMlpHidden)) =
+                make_uint4(packed[4], packed[5], packed[6], packed[7]);
         }
-        *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0, kMlpHidden)) =
-            make_uint4(packed[0], packed[1], packed[2], packed[3]);
-        *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0 + 8, kMlpHidden)) =
-            make_uint4(packed[4], packed[5], packed[6], packed[7]);
     }
 }
 
-// Persistent: each CTA (4 warps, one row per thread) loads the weights once and
-// runs 128-row tiles.  x: BF16 [rows][48] row-major; logits: FP32 [rows].
-__global__ void __launch_bounds__(128, 1)
+// Barrier of one 128-thread warp group (named barrier 1 + group).
+__device__ __forceinline__ void group_sync(int grp) {
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + grp) : "memory");
+}
+
+// Barrier of one warp group that also ORs a predicate over its threads.
+__device__ __forceinline__ bool group_sync_or(bool pred, int grp) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(1 + grp)
+        : "memory");
+    return r != 0;
+}
+
+// Persistent: each CTA loads the weights once; its two warp groups (4 warps,
+// one row per thread each) run independent streams of 128-row tiles, each with
+// its own X/H images, TMEM accumulator (columns 128 g ..) and mbarrier, so one
+// group's MMAs overlap the other's epilogue.  x: BF16 [rows][48] row-major;
+// logits: FP32 [rows].
+__global__ void __launch_bounds__(128 * kFwdGroups, 1)
     mlp_forward_kernel(const uint16_t* __restrict__ x, int rows, const int* __restrict__ rows_dev,
                        const uint4* __restrict__ images, const float* __restrict__ params, float* __restrict__ logits,
                        int* __restrict__ err) {
     // rows_dev (optional): the row count produced on the device, capped by rows.
     if (rows_dev) rows = min(rows, *rows_dev);
     extern __shared__ __align__(1024) uint8_t sm[];
-    const int t = threadIdx.x, warp = t >> 5;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar);
+    const int t = threadIdx.x, warp = t >> 5, grp = t >> 7, gt = t & 127;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar) + grp;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSmTmem);
     float* vec = reinterpret_cast<float*>(sm + kSmVec);
+    uint8_t* xs = sm + kSmGroup0 + grp * kSmGroupStride;
+    uint8_t* hs = xs + kImgW1;
 
     for (uint32_t i = t; i < kImagesBytes / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
     for (int i = t; i < kMlpHidden; i += blockDim.x) {
@@ -116,39 +150,39 @@ __global__ void __launch_bounds__(128, 1)
     }
     if (t == 0) {
         vec[4 * kMlpHidden] = params[kOffB4];
-        mbar_init(bar, 1);
+        for (int g = 0; g < kFwdGroups; ++g) mbar_init(reinterpret_cast<uint64_t*>(sm + kSmBar) + g, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) tc::tmem_alloc(tmem_slot, 128);
+    if (warp == 0) tc::tmem_alloc(tmem_slot, 128 * kFwdGroups);
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+    const uint32_t tmem = *tmem_slot + 128u * grp;
+    const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     const uint32_t idesc = tc::make_idesc_bf16(128, kMlpHidden, 0, 0);
     const uint32_t sbase = tc::smem_addr(sm);
     uint32_t phase = 0;
     bool bad = false;
 
     const int tiles = (rows + 127) / 128;
-    for (int tile = blockIdx.x; tile < tiles && !bad; tile += gridDim.x) {
-        const int row = tile * 128 + t;
+    for (int tile = blockIdx.x * kFwdGroups + grp; tile < tiles && !bad; tile += gridDim.x * kFwdGroups) {
+        const int row = tile * 128 + gt;
         // X tile: this thread's row, six 16-byte chunks of 8 features.
         const uint4* src = reinterpret_cast<const uint4*>(x + (size_t)row * kMlpIn);
 #pragma unroll
         for (int j = 0; j < kMlpIn / 8; ++j) {
             const uint4 v = row < rows ? src[j] : make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4*>(sm + kSmX + tc::cm_offset(t, 8 * j, kMlpIn)) = v;
+            *reinterpret_cast<uint4*>(xs + tc::cm_offset(gt, 8 * j, kMlpIn)) = v;
         }
-        // Three layers: MMAs from one thread, epilogue from all.
+        // Three layers: MMAs from the group's first thread, epilogue from all.
 #pragma unroll 1
         for (int layer = 0; layer < 3; ++layer) {
             tc::fence_async_smem();
             tc::fence_before();
-            __syncthreads();
-            if (t == 0) {
+            group_sync(grp);
+            if (gt == 0) {
                 tc::fence_after();
-                const uint32_t a0 = sbase + (layer == 0 ? kSmX : kSmH);
+                const uint32_t a0 = tc::smem_addr(layer == 0 ? xs : hs);
                 const uint32_t b0 = sbase + (layer == 0 ? kSmW1 : layer == 1 ? kSmW2 : kSmW3);
                 const int K = layer == 0 ? kMlpIn : kMlpHidden;
                 const uint32_t sbo = (uint32_t)(K / 8) * 128u;
@@ -158,35 +192,36 @@ __global__ void __launch_bounds__(128, 1)
                 tc::commit(bar);
             }
             const bool ok = mbar_wait_bounded(bar, phase, 1u << 22);
-            if (__syncthreads_or(!ok)) {  // CTA-uniform decision
+            if (group_sync_or(!ok, grp)) {  // group-uniform decision
                 bad = true;
                 break;
             }
             phase ^= 1u;
             tc::fence_after();
             if (layer < 2) {
-                epilogue_relu_to_smem(taddr, vec + layer * kMlpHidden, sm + kSmH, t);
+                epilogue_relu_to_smem(taddr, vec + layer * kMlpHidden, hs, gt);
             } else {
                 float acc = vec[4 * kMlpHidden];
 #pragma unroll 1
-                for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
-                    float v[16];
+                for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
+                    float v[32];
                     tc::tmem_ld16(taddr + c0, v);
+                    tc::tmem_ld16(taddr + c0 + 16, v + 16);
                     tc::wait_ld();
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
+                    for (int i = 0; i < 32; ++i)
                         acc = fmaf(fmaxf(v[i] + vec[2 * kMlpHidden + c0 + i], 0.0f), vec[3 * kMlpHidden + c0 + i], acc);
                 }
                 if (row < rows) logits[row] = acc;
             }
         }
     }
-    if (bad && t == 0) atomicOr(err, 1);
+    if (bad && gt == 0) atomicOr(err, 1);
     if (bad) mbar_wait_bounded(bar, phase, 1u << 22);  // let in-flight MMAs finish before freeing TMEM
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    if (warp == 0) tc::tmem_free(tmem, 128);
+    if (warp == 0) tc::tmem_free(*tmem_slot, 128 * kFwdGroups);
 }
 
 // ---------------------------------------------------------------- training
@@ -509,9 +544,11 @@ cudaError_t mlp_forward(const uint16_t* d_x, int rows, const uint8_t* d_images, 
     cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
     if (e != cudaSuccess) return e;
     const int tiles = (rows + 127) / 128;
-    const int grid = tiles < num_sms ? tiles : num_sms;
-    mlp_forward_kernel<<<grid, 128, kFwdSmem, st>>>(d_x, rows, d_rows, reinterpret_cast<const uint4*>(d_images),
-                                                     d_params, d_logits, d_err);
+    const int ctas = (tiles + kFwdGroups - 1) / kFwdGroups;
+    const int grid = ctas < num_sms ? ctas : num_sms;
+    mlp_forward_kernel<<<grid, 128 * kFwdGroups, kFwdSmem, st>>>(d_x, rows, d_rows,
+                                                                 reinterpret_cast<const uint4*>(d_images), d_params,
+                                                                 d_logits, d_err);
     return cudaGetLastError();
 }
 
