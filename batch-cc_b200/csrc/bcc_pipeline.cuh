@@ -631,11 +631,15 @@ __device__ __forceinline__ uint32_t record_bytes_of(float4 h1) {
 }
 
 // One CTA per (environment, edge tile): blockIdx.x = environment, blockIdx.y = tile.
-// Check CTAs are sized for 32 resident warps per SM (at most 64 registers).
-constexpr int kCheckWarpsPerSM = 32;
+// Check CTAs are compiled for M::check_warps_per_sm resident warps per SM (a
+// register budget of 65536 / (32 x that) per thread), at most 32 CTAs per SM.
+template <class M, int WARPS>
+constexpr int check_min_ctas() {
+    return M::check_warps_per_sm / WARPS < 32 ? M::check_warps_per_sm / WARPS : 32;
+}
 
 template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32, kCheckWarpsPerSM / WARPS) check_kernel(CheckParams P) {
+__global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ uint8_t s_perm[WARPS][kMaxSegments];
@@ -667,7 +671,7 @@ __global__ void __launch_bounds__(WARPS * 32, kCheckWarpsPerSM / WARPS) check_ke
 constexpr int kItemsPerGrab = 2;
 
 template <class M, int WARPS, int MODE>
-__global__ void __launch_bounds__(WARPS * 32, kCheckWarpsPerSM / WARPS) check_persistent_kernel(CheckParams P) {
+__global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_persistent_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ uint8_t s_perm[WARPS][kMaxSegments];

@@ -40,6 +40,12 @@ FK_FLOPS = {"panda": 1150, "fetch": 983, "baxter": 1792}
 # spheres, a check dominated by its walk) by 6 %.
 TABLE_TILE = {"panda": 1, "fetch": 32, "baxter": 32}
 
+# Resident warps per SM the check kernel is compiled for (its register budget
+# is 65536 / (32 x this)).  Measured on B200: Panda's check runs 4.6 % faster
+# at 40 (51 registers, a small spill) than at 32 (64 registers); Fetch's and
+# Baxter's longer overhang-aware walk runs 4-12 % slower at 40.
+CHECK_WARPS_PER_SM = {"panda": 40, "fetch": 32, "baxter": 32}
+
 
 def rpy_matrix(r, p, y):
     cr, sr = math.cos(r), math.sin(r)
@@ -89,6 +95,8 @@ def main():
     w("    static constexpr int fk_flops = %d;" % FK_FLOPS[name])
     w("    // Sample-table rows per tile (sphere-major inside a tile; 1 = row-major).")
     w("    static constexpr int table_tile = %d;" % TABLE_TILE[name])
+    w("    // Resident warps per SM the check kernel is compiled for (register budget).")
+    w("    static constexpr int check_warps_per_sm = %d;" % CHECK_WARPS_PER_SM[name])
     w("")
     w("    // Fixed transform of joint k (row-major 3x4: rotation | translation).")
     w("    // frame k+1 = frame joint_parent[k] * F_k * J_k(q_k), J = Rz(q) for a revolute")
