@@ -42,7 +42,7 @@ TABLE_TILE = {"panda": 1, "fetch": 32, "baxter": 32}
 
 # Resident warps per SM the check kernel is compiled for (its register budget
 # is 65536 / (32 x this)).  Measured on B200: Panda's check runs 4.6 % faster
-# at 40 (51 registers, a small spill) than at 32 (64 registers); Fetch's and
+# at 40 (48 registers, a small spill) than at 32 (64 registers); Fetch's and
 # Baxter's longer overhang-aware walk runs 4-12 % slower at 40.
 CHECK_WARPS_PER_SM = {"panda": 40, "fetch": 32, "baxter": 32}
 
