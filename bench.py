@@ -153,11 +153,29 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
+        if args.impl == "ours":  # the reference arm runs on the host cores (gloo), no GPU needed
+            torch.cuda.set_device(local)
         backend = "nccl" if args.impl == "ours" else "gloo"
         dist.init_process_group(backend, timeout=timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
+
+
+def rank_edges(workload_name_, num_edges, rank):
+    """Each rank checks its own seeded edge set against the same environments
+    (weak scaling: per-rank work fixed as ranks are added)."""
+    from bcc import workload
+    return workload.gen_edges(workload_name_, num_edges, seed=rank)
+
+
+def max_over_ranks(dist, v, device):
+    """The largest of every rank's value (identity without a process group)."""
+    if not dist:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cpu_baseline(envs, edges, robot="panda", target_s=12.0):
@@ -353,7 +371,7 @@ def run_ours(args, world, rank, local, dist):
     robot = workload.robot_of(args.workload)
     proposal = train_proposal(chk, args)
     envs = workload.gen_envs(args.workload, args.envs, seed=0)
-    edges = workload.gen_edges(args.workload, args.edges, seed=rank)
+    edges = rank_edges(args.workload, args.edges, rank)
     N, E = envs.num_envs, len(edges)
     chk.upload(envs)
     proposal.update(chk.mlp_evaluate(edges, 1 << 20, seed=7, robot=robot))
@@ -377,14 +395,7 @@ def run_ours(args, world, rank, local, dist):
                                         robot)
     torch.cuda.synchronize()
 
-    def max_over_ranks(v):
-        if not dist:
-            return v
-        t = torch.tensor([v], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    ms = {o: max_over_ranks(results[o][0]) / args.steps for o in results}
+    ms = {o: max_over_ranks(dist, results[o][0], f"cuda:{dev}") / args.steps for o in results}
     head = args.order
     value = world * N * E / (ms[head] * 1e-3)
 
@@ -421,7 +432,7 @@ def run_ours(args, world, rank, local, dist):
         t0 = time.perf_counter()
         chk.check(h_edges, out=h_res, order=head, robot=robot)
         t_e2e.append(time.perf_counter() - t0)
-    e2e_s = max_over_ranks(statistics.median(t_e2e))
+    e2e_s = max_over_ranks(dist, statistics.median(t_e2e), f"cuda:{dev}")
     mlp_ms, mlp_tf = mlp_roofline(chk, dev)
 
     if rank != 0:
