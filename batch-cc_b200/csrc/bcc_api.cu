@@ -156,11 +156,14 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     BCC_CUDA(ctx, ctx->edge_self.ensure(sizeof(int) * (size_t)E));
     const int G = ops->num_env_groups;
     BCC_CUDA(ctx, ctx->swept.ensure(sizeof(float4) * 2 * (size_t)G * E));
+    BCC_CUDA(ctx, ctx->edge_tri.ensure(sizeof(int) * (size_t)G * E));
     BCC_CUDA(ctx, ctx->error_flag.ensure(sizeof(int)));
     a.steps = ctx->steps.as<int>();
     a.offs = ctx->offs.as<int>();
     a.edge_self = ctx->edge_self.as<int>();
     a.swept = ctx->swept.as<float4>();
+    a.edge_tri = ctx->edge_tri.as<int>();
+    a.grid_bounds = ctx->grid_bounds.as<float>();
     a.error_flag = ctx->error_flag.as<int>();
     a.stage_events = ctx->profiling ? ctx->ev : nullptr;
     a.counters = nullptr;
@@ -490,45 +493,72 @@ struct Arena {
     std::vector<float> blob;     // concatenated blobs (float words, 16-byte granules)
     std::vector<float> hdr;      // [N][8]
     size_t max_record_bytes = 0;
+    // Cull grid shared by every environment of the set: slab s of axis a is
+    // [bnd[a][s], bnd[a][s + 1]).
+    float bnd[3][bcc::kGridSlabs + 1] = {};
 };
 
+// Largest slab s in [0, K) with bnd[s] <= x (0 below the first boundary);
+// the device lookup (swept_kernel) compares against the same floats.
+int slab_of(const float* bnd, double x) {
+    int s = 0;
+    for (int i = 1; i < bcc::kGridSlabs; ++i)
+        if ((double)bnd[i] <= x) s = i;
+    return s;
+}
+
+// One cull grid serves all environments of the set, so an edge's slab ranges
+// depend on the edge alone and are found once per edge (swept_kernel).  The
+// kGridSlabs slabs of an axis run from below every primitive AABB to above
+// them, split at quantiles of the primitives' centres: slabs are narrow where
+// primitives are dense.
 void build_arena(const std::vector<Rec>& recs, const std::vector<int>& off, Arena& A) {
     const int N = (int)off.size() - 1;
     constexpr int K = bcc::kGridSlabs;
     constexpr int TRI = bcc::kGridTri;
     A.blob.clear();
     A.hdr.assign((size_t)N * 8, 0.0f);
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> c;
+        double lo = 1e30, hi = -1e30;
+        c.reserve(recs.size());
+        for (const Rec& r : recs) {
+            c.push_back(r.v[a]);
+            lo = std::min(lo, (double)r.v[a] - r.v[16 + a]);
+            hi = std::max(hi, (double)r.v[a] + r.v[16 + a]);
+        }
+        float* b = A.bnd[a];
+        if (c.empty()) {
+            for (int i = 0; i <= K; ++i) b[i] = (float)i;
+            continue;
+        }
+        std::sort(c.begin(), c.end());
+        b[0] = std::nextafter((float)(lo - 1e-4), -INFINITY);
+        b[K] = std::nextafter((float)(hi + 1e-4), INFINITY);
+        for (int i = 1; i < K; ++i) {
+            const double q = c[std::min(c.size() - 1, (size_t)((double)i * c.size() / K))];
+            b[i] = std::min(std::max((float)q, std::nextafter(b[i - 1], INFINITY)), b[K]);
+        }
+        for (int i = K - 1; i >= 1; --i)  // strictly increasing up to b[K]
+            if (b[i] >= b[i + 1]) b[i] = std::nextafter(b[i + 1], -INFINITY);
+    }
     for (int i = 0; i < N; ++i) {
         const int p0 = off[i], np = off[i + 1] - off[i];
         const int W = np > 0 ? (np + 63) / 64 : 0;
         const size_t start = A.blob.size();  // in floats, multiple of 4
-        double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
         for (int p = 0; p < np; ++p) {
             const Rec& r = recs[p0 + p];
             for (int k = 0; k < 20; ++k) A.blob.push_back(r.v[k]);
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = std::min(lo[a], (double)r.v[a] - r.v[16 + a]);
-                hi[a] = std::max(hi[a], (double)r.v[a] + r.v[16 + a]);
-            }
         }
-        float inv[3] = {1.0f, 1.0f, 1.0f};
-        float org[3] = {0.0f, 0.0f, 0.0f};
         if (np > 0) {
-            for (int a = 0; a < 3; ++a) {
-                const double width = (hi[a] - lo[a]) / K;
-                org[a] = (float)lo[a];
-                inv[a] = width > 1e-9 ? (float)(1.0 / width) : 1.0f;
-            }
-            // Slab range of each primitive, widened by 1e-5 m so that the FP32 slab
-            // arithmetic on the device can only over-include.
+            // Slab range of each primitive's AABB, widened by 1e-5 m so that the
+            // FP32 swept boxes on the device can only over-include.
             std::vector<int> s0(3 * (size_t)np), s1(3 * (size_t)np);
             for (int p = 0; p < np; ++p) {
                 const Rec& r = recs[p0 + p];
                 for (int a = 0; a < 3; ++a) {
-                    const double l = ((double)r.v[a] - r.v[16 + a] - 1e-5 - org[a]) * inv[a];
-                    const double h = ((double)r.v[a] + r.v[16 + a] + 1e-5 - org[a]) * inv[a];
-                    s0[3 * p + a] = (int)std::min<double>(K - 1, std::max(0.0, std::floor(l)));
-                    s1[3 * p + a] = (int)std::min<double>(K - 1, std::max(0.0, std::floor(h)));
+                    s0[3 * p + a] = slab_of(A.bnd[a], (double)r.v[a] - r.v[16 + a] - 1e-5);
+                    s1[3 * p + a] = slab_of(A.bnd[a], (double)r.v[a] + r.v[16 + a] + 1e-5);
                 }
             }
             std::vector<uint64_t> m((size_t)3 * TRI * W, 0);
@@ -548,13 +578,7 @@ void build_arena(const std::vector<Rec>& recs, const std::vector<int>& off, Aren
         const uint32_t off16 = (uint32_t)(start / 4);  // float4 units
         const uint32_t shape = (uint32_t)np | ((uint32_t)W << 16);
         float* h = &A.hdr[(size_t)i * 8];
-        h[0] = org[0];
-        h[1] = org[1];
-        h[2] = org[2];
         std::memcpy(&h[3], &off16, 4);
-        h[4] = inv[0];
-        h[5] = inv[1];
-        h[6] = inv[2];
         std::memcpy(&h[7], &shape, 4);
     }
     if (A.blob.empty()) A.blob.assign(4, 0.0f);
@@ -601,6 +625,8 @@ bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
     ctx->num_envs = N;
     ctx->max_prims = max_prims;
     ctx->blob_smem = blob_smem;
+    BCC_CUDA(ctx, ctx->grid_bounds.ensure(sizeof(A.bnd)));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->grid_bounds.p, A.bnd, sizeof(A.bnd), cudaMemcpyHostToDevice));
     ctx->env_code_ready = false;
     ctx->env_version += 1;
     return BCC_OK;

@@ -78,6 +78,7 @@ struct bcc_ctx {
     int num_envs = -1;
     int max_prims = 0;
     size_t blob_smem = 0;
+
     bcc::DevBuf blobs, env_hdr;
     // per-call buffers
     bcc::DevBuf edges, steps, offs, table, row_edge, edge_self, swept, results, error_flag;
@@ -88,6 +89,8 @@ struct bcc_ctx {
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     // learned proposal
     bcc::MlpState mlp;
+    bcc::DevBuf edge_tri;    // [E][groups] packed slab ranges of each group's swept box
+    bcc::DevBuf grid_bounds; // [3][kGridSlabs + 1] slab boundaries of the uploaded set's cull grid
     bcc::DevBuf env_code;    // [num_envs][32] environment encodings
     bool env_code_ready = false;
     bcc::DevBuf q_count, q_edges, q_rows;  // learned-order queue of undecided pairs

@@ -7,9 +7,10 @@
 
 namespace bcc {
 
-// Cull grid of an environment: kGridSlabs slabs per axis between the min and
-// max of its primitives' AABBs; for every slab range [i0, i1] (triangular
-// index) a bit mask of the primitives whose AABB meets that range.
+// Cull grid of an environment set: kGridSlabs slabs per axis (boundaries at
+// quantiles of the primitives' centres); per environment and slab range
+// [i0, i1] (triangular index) a bit mask of the primitives whose AABB meets
+// that range.
 constexpr int kGridSlabs = 32;
 constexpr int kGridTri = kGridSlabs * (kGridSlabs + 1) / 2;
 
@@ -31,6 +32,7 @@ struct CheckParams {
     const int* offs;         // [E + 1] first sample row of each edge
     const float4* table;     // [rows][num_spheres] sphere centres + radius
     const float4* swept;     // [E][groups][2] cull AABB centre / half-size
+    const int* edge_tri;     // [E][groups] slab ranges on the set's grid (tx | ty << 10 | tz << 20), -1 = none
     const int* edge_self;    // [E] 1 when some sample self-collides
     uint8_t* results;        // [E][num_envs]
     int* error_flag;         // set when a bounded wait gives up
@@ -68,6 +70,8 @@ struct PipelineArgs {
     int* row_edge;           // [total_rows]
     int* edge_self;          // [E]
     float4* swept;           // [E][groups][2]
+    int* edge_tri;           // [E][groups], null = not needed (records check)
+    const float* grid_bounds;  // [3][kGridSlabs + 1] cull-grid slab boundaries of the environment set
     const float4* blobs;
     const float4* env_hdr;
     int num_envs;
@@ -167,6 +171,7 @@ inline CheckParams params_of(const PipelineArgs& a) {
     P.offs = a.offs;
     P.table = a.table;
     P.swept = a.swept;
+    P.edge_tri = a.edge_tri;
     P.edge_self = a.edge_self;
     P.results = a.d_results;
     P.error_flag = a.error_flag;

@@ -236,54 +236,91 @@ __global__ void __launch_bounds__(kSelfThreads) self_kernel(const float4* __rest
 }
 
 // ------------------------------------------------------------------ 5. swept
-// One warp per edge: AABB (lo, hi) of every env group's bounding sphere over
+// Slab of x on one axis: the largest s in [0, kGridSlabs) with b[s] <= x (0
+// below b[0]); b holds the axis' kGridSlabs + 1 increasing boundaries.
+__device__ __forceinline__ int slab_of(const float* __restrict__ b, float x) {
+    int s = 0;
+#pragma unroll
+    for (int step = kGridSlabs / 2; step; step >>= 1)
+        if (b[s + step] <= x) s += step;
+    return s;
+}
+
+// Slab index range of [lo, hi] on one axis of the environment set's cull grid,
+// as a triangular table index; -1 when the interval misses every primitive.
+__device__ __forceinline__ int slab_tri(float lo, float hi, const float* __restrict__ b) {
+    if (!(hi >= b[0]) || !(lo < b[kGridSlabs])) return -1;
+    return tri_index(slab_of(b, lo), slab_of(b, hi));
+}
+
+// One warp per edge: AABB (lo, hi) of every link group's bounding sphere over
 // the edge's samples, inflated by radius + 0.005 + the group's leaf overhang +
-// cull margin.
+// cull margin; and (edge_tri non-null) its slab ranges on the set's cull grid,
+// packed tx | ty << 10 | tz << 20 (-1 when some axis misses every primitive).
+// Lane g ends up holding group g's box.  Row-major tables: lane g scans group
+// g's bound down the rows (a row's bounds are contiguous).  Tiled tables: the
+// lanes scan 32 rows of one group at a time (contiguous in a tile) and a
+// butterfly reduction hands the box to lane g.
 template <class M>
 __global__ void swept_kernel(const float4* __restrict__ table, const int* __restrict__ offs, int E,
-                             float4* __restrict__ swept) {
+                             float4* __restrict__ swept, int* __restrict__ edge_tri,
+                             const float* __restrict__ bounds) {
+    constexpr int G = M::num_env_groups;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= E) return;
     const int r0 = offs[warp], r1 = offs[warp + 1];
     const DevTables<M>& T = tab<M>();
-    for (int g = 0; g < M::num_env_groups; ++g) {
-        const int b = g;  // bounds lead every table row
-        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int r = r0 + lane; r < r1; r += 32) {
-            const float4 c = table[table_index<M>(r, b)];
-            lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
-            hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
-        }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = fminf(lo[a], __shfl_xor_sync(kFull, lo[a], o));
-                hi[a] = fmaxf(hi[a], __shfl_xor_sync(kFull, hi[a], o));
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if constexpr (M::table_tile == 1) {
+        if (lane < G) {
+            for (int r = r0; r < r1; ++r) {
+                const float4 c = table[table_index<M>(r, lane)];  // bounds lead every table row
+                lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
+                hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
             }
         }
-        if (lane == 0) {
-            const float pad = T.sphere_radius[b] + kEnvInflate + T.cull_pad[g] + kCullMargin;
-            const float4 l = make_float4(lo[0] - pad, lo[1] - pad, lo[2] - pad, 0.0f);
-            const float4 h = make_float4(hi[0] + pad, hi[1] + pad, hi[2] + pad, 0.0f);
-            swept[((size_t)warp * M::num_env_groups + g) * 2 + 0] = l;
-            swept[((size_t)warp * M::num_env_groups + g) * 2 + 1] = h;
+    } else {
+        for (int g = 0; g < G; ++g) {
+            float l3[3] = {INFINITY, INFINITY, INFINITY}, h3[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (int r = r0 + lane; r < r1; r += 32) {
+                const float4 c = table[table_index<M>(r, g)];
+                l3[0] = fminf(l3[0], c.x); l3[1] = fminf(l3[1], c.y); l3[2] = fminf(l3[2], c.z);
+                h3[0] = fmaxf(h3[0], c.x); h3[1] = fmaxf(h3[1], c.y); h3[2] = fmaxf(h3[2], c.z);
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    l3[a] = fminf(l3[a], __shfl_xor_sync(kFull, l3[a], o));
+                    h3[a] = fmaxf(h3[a], __shfl_xor_sync(kFull, h3[a], o));
+                }
+            }
+            if (lane == g) {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = l3[a];
+                    hi[a] = h3[a];
+                }
+            }
         }
+    }
+    if (lane >= G) return;
+    const int g = lane;
+    const float pad = T.sphere_radius[g] + kEnvInflate + T.cull_pad[g] + kCullMargin;
+    const float4 l = make_float4(lo[0] - pad, lo[1] - pad, lo[2] - pad, 0.0f);
+    const float4 h = make_float4(hi[0] + pad, hi[1] + pad, hi[2] + pad, 0.0f);
+    swept[((size_t)warp * G + g) * 2 + 0] = l;
+    swept[((size_t)warp * G + g) * 2 + 1] = h;
+    if (edge_tri) {
+        const int tx = slab_tri(l.x, h.x, bounds);
+        const int ty = slab_tri(l.y, h.y, bounds + (kGridSlabs + 1));
+        const int tz = slab_tri(l.z, h.z, bounds + 2 * (kGridSlabs + 1));
+        edge_tri[(size_t)warp * G + g] = (tx < 0 || ty < 0 || tz < 0) ? -1 : (tx | (ty << 10) | (tz << 20));
     }
 }
 
 // ------------------------------------------------------------------ 6. check
-// Slab index range of [lo, hi] on one axis of an environment's cull grid, as a
-// triangular table index; -1 when the interval misses every primitive.
-__device__ __forceinline__ int slab_tri(float lo, float hi, float g0, float inv) {
-    const float f0 = (lo - g0) * inv, f1 = (hi - g0) * inv;
-    if (!(f1 >= 0.0f) || !(f0 < (float)kGridSlabs)) return -1;
-    const int i0 = (int)fminf(fmaxf(floorf(f0), 0.0f), (float)(kGridSlabs - 1));
-    const int i1 = (int)fminf(fmaxf(floorf(f1), 0.0f), (float)(kGridSlabs - 1));
-    return tri_index(i0, i1);
-}
-
 // Whole warp: does link group g's bounding sphere at sample k hit any of the
 // environment's np primitives (the reference's gate, every primitive)?
 template <class M>
@@ -503,24 +540,22 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
             if (lane == 0) *out = self ? 1 : 0;
             continue;
         }
-        // Cull: lane g < G intersects link g's swept box with the env's slab tables.
-        int tx = -1, ty = -1, tz = -1;
-        if (lane < G) {
-            const float4 lo = P.swept[((size_t)e * G + lane) * 2 + 0];
-            const float4 hi = P.swept[((size_t)e * G + lane) * 2 + 1];
-            tx = slab_tri(lo.x, hi.x, h0.x, h1.x);
-            ty = slab_tri(lo.y, hi.y, h0.y, h1.y);
-            tz = slab_tri(lo.z, hi.z, h0.z, h1.z);
-        }
-        const bool live = tx >= 0 && ty >= 0 && tz >= 0;
+        // Cull: lane g < G takes link g's slab ranges on the set's grid (computed
+        // once per edge) and ANDs the environment's three masks over them.
+        const int code = lane < G ? P.edge_tri[(size_t)e * G + lane] : -1;
+        // Word w of link g's candidate mask (only the packed code stays live
+        // across the walk; the three offsets are re-derived where needed).
+        auto mask_word = [&](int w) {
+            const int tx = code & 1023, ty = (code >> 10) & 1023, tz = code >> 20;
+            return __ldg(masks + tx * W + w) & __ldg(masks + (kGridTri + ty) * W + w) &
+                   __ldg(masks + (2 * kGridTri + tz) * W + w);
+        };
         // Compact the surviving (primitive, link) pairs, link-major: lane g counts
         // link g's candidates, an exclusive warp scan gives each link its offset,
         // and every lane writes its own link's pairs in primitive order.
-        const int ox = (live ? tx : 0) * W, oy = (kGridTri + (live ? ty : 0)) * W,
-                  oz = (2 * kGridTri + (live ? tz : 0)) * W;
         int cnt = 0;
-        if (live)
-            for (int w = 0; w < W; ++w) cnt += __popcll(__ldg(masks + ox + w) & __ldg(masks + oy + w) & __ldg(masks + oz + w));
+        if (code >= 0)
+            for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
         int off = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -538,7 +573,7 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
             if (cnt > 0 && off < seg1 && off + cnt > seg0) {
                 int idx = off;
                 for (int w = 0; w < W && idx < seg1; ++w) {
-                    uint64_t m = __ldg(masks + ox + w) & __ldg(masks + oy + w) & __ldg(masks + oz + w);
+                    uint64_t m = mask_word(w);
                     while (m && idx < seg1) {
                         const int b = __ffsll((long long)m) - 1;
                         if (idx >= seg0) pairs[idx - seg0] = (uint16_t)(((w * 64 + b) << GB) | lane);
@@ -999,7 +1034,8 @@ cudaError_t run_prep(const PipelineArgs& a, cudaStream_t st) {
         self_kernel<M><<<grid, kSelfThreads, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
     }
     if (ev) cudaEventRecord(ev[3], st);
-    swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept);
+    swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept,
+                                                           a.grid_bounds ? a.edge_tri : nullptr, a.grid_bounds);
     if (ev) cudaEventRecord(ev[4], st);
     return cudaGetLastError();
 }
