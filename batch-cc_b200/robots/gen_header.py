@@ -41,10 +41,11 @@ FK_FLOPS = {"panda": 1150, "fetch": 983, "baxter": 1792}
 TABLE_TILE = {"panda": 1, "fetch": 32, "baxter": 32}
 
 # Resident warps per SM the check kernel is compiled for (its register budget
-# is 65536 / (32 x this)).  Measured on B200: Panda's check runs 4.6 % faster
-# at 40 (48 registers, a small spill) than at 32 (64 registers); Fetch's and
-# Baxter's longer overhang-aware walk runs 4-12 % slower at 40.
-CHECK_WARPS_PER_SM = {"panda": 40, "fetch": 32, "baxter": 32}
+# is 65536 / (32 x this)).  Swept on B200 (uneven / multi workloads, autotuned
+# launch shapes): Panda 48 (42 registers) beats 40 by 2 % and 32 by 10 %;
+# Fetch's overhang-aware walk is best at 32 (64 registers); Baxter's at 28
+# (73 registers, 4-warp CTAs) beats 32 by 3 %.
+CHECK_WARPS_PER_SM = {"panda": 48, "fetch": 32, "baxter": 28}
 
 
 def rpy_matrix(r, p, y):
