@@ -227,42 +227,46 @@ constexpr int kLearnedRowCap = 16 << 20;  // MLP rows per learned check (1.5 GB 
 // MLP scores; (3) the queued pairs walked in descending segment score.
 // Buffers are sized here, outside any stream capture.
 bcc_status prepare_learned(bcc_ctx* ctx, bcc::PipelineArgs& a) {
-    const int grid = bcc::check_grid_size(a);
-    const size_t qn = (size_t)grid * a.edges_per_cta;
-    BCC_CUDA(ctx, ctx->q_count.ensure(sizeof(int) * (size_t)grid + 64));
-    BCC_CUDA(ctx, ctx->q_edges.ensure(sizeof(int) * qn));
-    BCC_CUDA(ctx, ctx->q_rows.ensure(sizeof(int) * qn));
     const long long cap_ll = (long long)a.num_envs * (a.total_rows / bcc::kSegment) + 64;
     const int cap = (int)std::min<long long>(cap_ll, kLearnedRowCap);
+    // A queued pair takes at least 4 rows; the probe stops queueing once the
+    // rows are spent, so the queue needs cap / 4 entries plus the pairs that
+    // were in flight at that moment (the kernel checks the capacity anyway).
+    const long long pairs = (long long)a.num_envs * a.num_edges;
+    const int q_cap = (int)std::min<long long>(pairs, cap / 4 + (1 << 18));
+    BCC_CUDA(ctx, ctx->q_head.ensure(64));
+    BCC_CUDA(ctx, ctx->q_pairs.ensure(sizeof(int2) * (size_t)q_cap));
+    BCC_CUDA(ctx, ctx->q_rows.ensure(sizeof(int) * (size_t)q_cap));
     BCC_CUDA(ctx, ctx->mlp.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)cap));
     BCC_CUDA(ctx, ctx->mlp.logits.ensure(sizeof(float) * (size_t)cap));
-    a.q_count = ctx->q_count.as<int>();
-    a.row_count = a.q_count + grid;  // one counter past the per-CTA counts
-    a.q_edges = ctx->q_edges.as<int>();
+    a.q_head = ctx->q_head.as<unsigned long long>();
+    a.q_pairs = ctx->q_pairs.as<int2>();
     a.q_rows = ctx->q_rows.as<int>();
+    a.q_cap = q_cap;
     a.row_cap = cap;
     a.logits = ctx->mlp.logits.as<float>();
     a.queue_min_items = ctx->tune.queue_min_items;
-    ctx->learned_rows_dev = a.row_count;
+    a.finish_counter = a.work_counter + 1;
+    ctx->learned_rows_dev = reinterpret_cast<int*>(a.q_head);  // the low word counts rows
     ctx->learned_row_cap = cap;
     return BCC_OK;
 }
 
 bcc_status run_learned(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::PipelineArgs& a, cudaStream_t st) {
-    const int grid = bcc::check_grid_size(a);
-    BCC_CUDA(ctx, cudaMemsetAsync(a.q_count, 0, sizeof(int) * ((size_t)grid + 1), st));
+    BCC_CUDA(ctx, cudaMemsetAsync(a.q_head, 0, sizeof(unsigned long long), st));
     cudaEvent_t* ev = a.stage_events;
     BCC_CUDA(ctx, ops->prep(a, st));  // records stage events 1-4
     a.mode = 1;
     BCC_CUDA(ctx, ops->check_mode(a, st));
-    // No host round trip: the feature kernel reads the queue and the MLP
-    // kernel reads the device row count (capped by the buffer capacity).
-    BCC_CUDA(ctx, ops->queue_features(a, ctx->env_code.as<float>(), ctx->mlp.x.as<uint16_t>(), grid, st));
+    // No host round trip: the feature and finish kernels read the queue length
+    // and the MLP kernel the row count on the device (capped by the capacities).
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    BCC_CUDA(ctx, ops->queue_features(a, ctx->env_code.as<float>(), ctx->mlp.x.as<uint16_t>(), 16 * std::max(sms, 1),
+                                      st));
     BCC_CUDA(ctx, bcc::mlp_forward(ctx->mlp.x.as<uint16_t>(), a.row_cap, ctx->mlp.images.as<uint8_t>(),
                                    ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
-                                   std::max(sms, 1), st, a.row_count));
+                                   std::max(sms, 1), st, reinterpret_cast<const int*>(a.q_head)));
     a.mode = 2;
     BCC_CUDA(ctx, ops->check_mode(a, st));
     if (ev) cudaEventRecord(ev[5], st);
@@ -864,9 +868,9 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
                 }
             }
     if (s == BCC_OK && order == BCC_ORDER_LEARNED && ctx->mlp.ready) {
-        const int qmins[5] = {32, 64, 128, 256, 512};
+        const int qmins[6] = {64, 128, 256, 512, 1024, 2048};
         bcc::Tune base = best;
-        for (int qi = 0; qi < 5 && s == BCC_OK; ++qi) {
+        for (int qi = 0; qi < 6 && s == BCC_OK; ++qi) {
             bcc::Tune t = base;
             t.queue_min_items = qmins[qi];
             float ms = 0;

@@ -93,7 +93,7 @@ struct bcc_ctx {
     bcc::DevBuf grid_bounds; // [3][kGridSlabs + 1] slab boundaries of the uploaded set's cull grid
     bcc::DevBuf env_code;    // [num_envs][32] environment encodings
     bool env_code_ready = false;
-    bcc::DevBuf q_count, q_edges, q_rows;  // learned-order queue of undecided pairs
+    bcc::DevBuf q_head, q_pairs, q_rows;   // learned-order queue of undecided pairs
     const int* learned_rows_dev = nullptr; // device row count of the last learned check
     int learned_row_cap = 0;
     bcc::Tune tune;                        // launch configuration (autotuned or default)

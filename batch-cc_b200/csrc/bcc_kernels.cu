@@ -86,10 +86,6 @@ size_t records_smem_bytes(int max_prims, int groups, int warps) {
     return (size_t)max_prims * kPrimF4 * 16 + (size_t)warps * ppw * sizeof(uint16_t);
 }
 
-int check_grid_size(const PipelineArgs& a) {
-    return a.num_envs * ((a.num_edges + a.edges_per_cta - 1) / a.edges_per_cta);
-}
-
 // ------------------------------------------------------------------ environment code
 // 32-value environment code (one warp per environment): [0..3] counts of
 // sphere-like, capsule-like and box-like primitives and the total, / 64;

@@ -37,14 +37,15 @@ struct CheckParams {
     uint8_t* results;        // [E][num_envs]
     int* error_flag;         // set when a bounded wait gives up
     unsigned long long* counters;  // null, or kNumCounters work counters (diagnostics)
-    // Learned order (modes 1 and 2 of the check kernel); unused in plain mode.
-    int* q_count;            // [grid] queued edges of each CTA
-    int* q_edges;            // [grid][edges_per_cta] queued edge ids
-    int* q_rows;             // [grid][edges_per_cta] first MLP row of the entry, -1 = none
-    int* row_count;          // rows handed out so far
+    // Learned order (probe and finish); unused in plain mode.
+    unsigned long long* q_head;  // queue entries handed out << 32 | MLP rows handed out
+    int2* q_pairs;           // [q_cap] queued (edge, environment)
+    int* q_rows;             // [q_cap] first MLP row of the entry, -1 = none (the probe walked on)
+    int q_cap;               // capacity of the queue arrays
     int row_cap;             // capacity of the MLP row buffers
-    const float* logits;     // [row_cap] segment scores (mode 2)
+    const float* logits;     // [row_cap] segment scores (finish)
     int queue_min_items;     // probe: queue only pairs with at least this many items left
+    int* finish_counter;     // next queue entry for the finish kernel
     int persistent;          // 1: persistent kernel pulling work items from work_counter
     int* work_counter;
 };
@@ -84,13 +85,14 @@ struct PipelineArgs {
     cudaEvent_t* stage_events;  // null, or 6 events bracketing the 5 stages
     unsigned long long* counters;
     int mode;                // 0 plain, 1 probe (first chunk, queue the rest), 2 finish (learned order)
-    int* q_count;
-    int* q_edges;
+    unsigned long long* q_head;
+    int2* q_pairs;
     int* q_rows;
-    int* row_count;
+    int q_cap;
     int row_cap;
     const float* logits;
     int queue_min_items;
+    int* finish_counter;
     int persistent;
     int* work_counter;
 };
@@ -154,7 +156,6 @@ const RobotOps* robot_ops(int robot);
 // Robot-independent kernels (bcc_kernels.cu).
 cudaError_t launch_scan(const int* steps, int E, int* offs, cudaStream_t st);
 cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st);
-int check_grid_size(const PipelineArgs& a);
 size_t check_smem_bytes(int max_prims, int groups, size_t blob_smem, int warps);
 size_t records_smem_bytes(int max_prims, int groups, int warps);
 
@@ -176,13 +177,14 @@ inline CheckParams params_of(const PipelineArgs& a) {
     P.results = a.d_results;
     P.error_flag = a.error_flag;
     P.counters = a.counters;
-    P.q_count = a.q_count;
-    P.q_edges = a.q_edges;
+    P.q_head = a.q_head;
+    P.q_pairs = a.q_pairs;
     P.q_rows = a.q_rows;
-    P.row_count = a.row_count;
+    P.q_cap = a.q_cap;
     P.row_cap = a.row_cap;
     P.logits = a.logits;
     P.queue_min_items = a.queue_min_items;
+    P.finish_counter = a.finish_counter;
     P.persistent = a.persistent;
     P.work_counter = a.work_counter;
     return P;

@@ -358,16 +358,18 @@ __device__ __forceinline__ GroupLanes group_lanes() {
 
 // Whole warp: walk (sample rank, pair) items 32 at a time in check order --
 // plain reference order, or with `perm` the edge's segments in learned order --
-// and return whether some item collides.  MODE 1 (probe) stops after the
-// first chunk and sets `undecided` when at least queue_min_items remain.
+// and return whether some item collides.  MODE 1 (probe): after the first
+// chunk, when at least queue_min_items remain, the whole warp calls queue();
+// if that queues the pair, the walk stops with `undecided` set, otherwise it
+// goes on in plain order.
 // Each chunk tests the bounds (one per item); the leaf work of the items whose
 // bound hit is then flattened over the warp (item j owns leaf slots
 // [incl_j - cnt_j, incl_j)) and the warp stops at the first step with a hit.
-template <class M, int MODE>
+template <class M, int MODE, class Queue>
 __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, size_t row0, int n, int C,
                                            const uint16_t* pairs, const float4* prim, int np, const uint8_t* perm,
                                            int queue_min_items, const GroupLanes& GL, bool& undecided,
-                                           WalkStats& st) {
+                                           WalkStats& st, Queue&& queue) {
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
     constexpr bool kOver = has_overhang<M>();
@@ -489,7 +491,7 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
         }
         // Probe: after the first chunk, queue the pair for the learned order
         // only when much work remains; small remainders finish in plain order.
-        if (MODE == 1 && w0 == 0 && total - 32 >= queue_min_items) {
+        if (MODE == 1 && w0 == 0 && total - 32 >= queue_min_items && queue()) {
             undecided = true;
             break;
         }
@@ -503,23 +505,161 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
     return collide;
 }
 
-// MODE 0: plain order, full walk.  MODE 1 (learned pipeline, phase 1): plain
-// order, first 32-item chunk only; a pair still undecided after it is queued
-// (with MLP rows for its segments) instead of getting a verdict.  MODE 2
-// (phase 3): the CTA's queued pairs, walked in descending segment score.
-//
-// check_tile processes the edges of one (environment, edge tile) work item
-// with the environment's blob already staged in shared memory; it is shared
-// by the one-CTA-per-item grid kernel and the persistent kernel.
-template <class M, int WARPS, int MODE>
-__device__ __forceinline__ void check_tile(const CheckParams& P, int env, int tile, int n_slots,
-                                           const unsigned char* smem, uint8_t (*s_perm)[kMaxSegments], float4 h0,
-                                           float4 h1) {
+// Learned-order queue: lane 0 of a probing warp reserves a queue entry and the
+// 4 n MLP rows of the pair's segments with one 64-bit atomic on q_head (entries
+// in the high word, rows in the low word).  Returns the pair's first MLP row,
+// or -1 when the pair keeps the plain order (more than kMaxSegments segments,
+// or the row budget or the queue spent) and the probe walks on.  The low word
+// only grows while it is at most row_cap, so it stays far below 2^32.
+__device__ __forceinline__ int queue_pair(const CheckParams& P, int e, int env, int n) {
+    const int rows = 4 * n;
+    if (rows > kMaxSegments) return -1;
+    const unsigned used = *reinterpret_cast<volatile const unsigned*>(P.q_head);
+    if ((long long)used + rows > P.row_cap) return -1;
+    const unsigned long long old = atomicAdd(P.q_head, (1ull << 32) | (unsigned long long)rows);
+    const long long idx = (long long)(old >> 32);
+    if (idx >= P.q_cap) return -1;
+    const unsigned ro = (unsigned)old;
+    const int r = (long long)ro + rows <= P.row_cap ? (int)ro : -1;
+    P.q_pairs[idx] = make_int2(e, env);
+    P.q_rows[idx] = r;
+    return r;
+}
+
+// One (environment, edge) pair, whole warp: cull, pair-list compaction and the
+// walk.  MODE 0: plain order, full walk.  MODE 1 (learned pipeline, phase 1):
+// plain order; a pair still undecided after its first 32-item chunk may be
+// queued (with MLP rows for its segments) instead of getting a verdict.  MODE 2
+// (phase 3): a queued pair (first MLP row seg_row) walked in descending
+// segment score.  `prim` holds the environment's records (shared or global
+// memory), `masks` its cull masks, W 64-bit words per mask.
+template <class M, int MODE>
+__device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e, int seg_row, const float4* prim,
+                                           const uint64_t* __restrict__ masks, int np, int W, uint16_t* pairs,
+                                           uint8_t* perm_buf, const GroupLanes& GL) {
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
+    const int lane = threadIdx.x & 31;
+    const int K = P.pairs_per_warp;
+    uint8_t* out = P.results + (size_t)e * P.num_envs + env;
+    const int self = P.edge_self[e];
+    if (np == 0 || self) {  // a self-colliding sample collides in every environment
+        if (lane == 0) *out = self ? 1 : 0;
+        return;
+    }
+    // Cull: lane g < G takes link g's slab ranges on the set's grid (computed
+    // once per edge) and ANDs the environment's three masks over them.
+    const int code = lane < G ? P.edge_tri[(size_t)e * G + lane] : -1;
+    // Word w of link g's candidate mask (only the packed code stays live
+    // across the walk; the three offsets are re-derived where needed).
+    auto mask_word = [&](int w) {
+        const int tx = code & 1023, ty = (code >> 10) & 1023, tz = code >> 20;
+        return __ldg(masks + tx * W + w) & __ldg(masks + (kGridTri + ty) * W + w) &
+               __ldg(masks + (2 * kGridTri + tz) * W + w);
+    };
+    // Compact the surviving (primitive, link) pairs, link-major: lane g counts
+    // link g's candidates, an exclusive warp scan gives each link its offset,
+    // and every lane writes its own link's pairs in primitive order.
+    int cnt = 0;
+    if (code >= 0)
+        for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
+    int off = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, off, o);
+        if (lane >= o) off += y;
+    }
+    const int C = __shfl_sync(kFull, off, 31);
+    off -= cnt;
+
+    bool collide = false, undecided = false;
+    WalkStats st;
+    // Pair list entries [seg0, seg1): lane g writes link g's candidates that
+    // fall in the range.
+    auto write_seg = [&](int seg0, int seg1) {
+        if (cnt > 0 && off < seg1 && off + cnt > seg0) {
+            int idx = off;
+            for (int w = 0; w < W && idx < seg1; ++w) {
+                uint64_t m = mask_word(w);
+                while (m && idx < seg1) {
+                    const int b = __ffsll((long long)m) - 1;
+                    if (idx >= seg0) pairs[idx - seg0] = (uint16_t)(((w * 64 + b) << GB) | lane);
+                    ++idx;
+                    m &= m - 1;
+                }
+            }
+        }
+        __syncwarp();
+    };
+    auto queue = [&]() {
+        int ro = -1;
+        if (lane == 0) ro = queue_pair(P, e, env, P.steps[e]);
+        return __shfl_sync(kFull, ro, 0) >= 0;
+    };
+    auto walk_seg = [&](int Cs) {
+        const int n = P.steps[e];
+        const size_t row0 = (size_t)P.offs[e];
+        // Learned order: rank the edge's 4 n segments by their MLP score
+        // (descending, ties by index; NaN scores last).
+        const int nseg = 4 * n;
+        const bool learned = MODE == 2 && seg_row >= 0 && nseg <= kMaxSegments;
+        if (learned) {
+            float v0 = lane < nseg ? P.logits[seg_row + lane] : -INFINITY;
+            float v1 = lane + 32 < nseg ? P.logits[seg_row + lane + 32] : -INFINITY;
+            v0 = isnan(v0) ? -INFINITY : v0;
+            v1 = isnan(v1) ? -INFINITY : v1;
+            int rank0 = 0, rank1 = 0;
+            for (int i = 0; i < nseg; ++i) {
+                const float vi = __shfl_sync(kFull, i < 32 ? v0 : v1, i & 31);
+                rank0 += (vi > v0 || (vi == v0 && i < lane)) ? 1 : 0;
+                rank1 += (vi > v1 || (vi == v1 && i < lane + 32)) ? 1 : 0;
+            }
+            if (lane < nseg) perm_buf[rank0] = (uint8_t)lane;
+            if (lane + 32 < nseg) perm_buf[rank1] = (uint8_t)(lane + 32);
+            __syncwarp();
+        }
+        collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np, learned ? perm_buf : nullptr,
+                                      P.queue_min_items, GL, undecided, st, queue);
+        __syncwarp();  // every lane is done with this segment's pairs
+    };
+    // Robots whose leaves all lie inside their bounds have a small walk: a
+    // separate copy for the usual single-segment case keeps the segment
+    // bookkeeping out of it.  The overhang-aware walk stays in one copy.
+    bool single = false;
+    if constexpr (!has_overhang<M>()) single = C > 0 && C <= K;
+    if (single) {
+        write_seg(0, C);
+        walk_seg(C);
+    } else {
+        for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
+            const int seg1 = min(C, seg0 + K);
+            write_seg(seg0, seg1);
+            walk_seg(seg1 - seg0);
+        }
+    }
+    if (MODE == 1 && undecided) return;  // queued: the finish pass writes the verdict
+    if (lane == 0) {
+        *out = collide ? 1 : 0;
+        if (P.counters) {
+            atomicAdd(P.counters + 0, 1ull);
+            atomicAdd(P.counters + 1, (unsigned long long)C);
+            atomicAdd(P.counters + 2, st.chunks);
+            atomicAdd(P.counters + 3, st.gates);
+            atomicAdd(P.counters + 4, st.leaf);
+            atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
+        }
+    }
+}
+
+// check_tile processes the edges of one (environment, edge tile) work item
+// (modes 0 and 1) with the environment's records already staged in shared
+// memory; it is shared by the one-CTA-per-item grid kernel and the persistent
+// kernel.
+template <class M, int WARPS, int MODE>
+__device__ __forceinline__ void check_tile(const CheckParams& P, int env, int tile, int n_slots,
+                                           const unsigned char* smem, float4 h0, float4 h1) {
     const int e_begin = tile * P.edges_per_cta;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cta = tile * P.num_envs + env;
+    const int warp = threadIdx.x >> 5;
     const uint32_t shape = __float_as_uint(h1.w);
     const int np = (int)(shape & 0xffffu);
     const int W = (int)(shape >> 16);  // 64-bit words per primitive mask
@@ -528,134 +668,14 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
     // only the few words its slab ranges select
     const uint64_t* __restrict__ masks =
         reinterpret_cast<const uint64_t*>(P.blobs + (size_t)__float_as_uint(h0.w) + (size_t)np * kPrimF4);
-    const int K = P.pairs_per_warp;
-    uint16_t* pairs = reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) + (size_t)warp * K;
+    uint16_t* pairs =
+        reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) + (size_t)warp * P.pairs_per_warp;
     const GroupLanes GL = group_lanes<M>();
-
-    for (int slot = warp; slot < n_slots; slot += WARPS) {
-        const int e = MODE == 2 ? P.q_edges[(size_t)cta * P.edges_per_cta + slot] : e_begin + slot;
-        uint8_t* out = P.results + (size_t)e * P.num_envs + env;
-        const int self = P.edge_self[e];
-        if (np == 0 || self) {  // a self-colliding sample collides in every environment
-            if (lane == 0) *out = self ? 1 : 0;
-            continue;
-        }
-        // Cull: lane g < G takes link g's slab ranges on the set's grid (computed
-        // once per edge) and ANDs the environment's three masks over them.
-        const int code = lane < G ? P.edge_tri[(size_t)e * G + lane] : -1;
-        // Word w of link g's candidate mask (only the packed code stays live
-        // across the walk; the three offsets are re-derived where needed).
-        auto mask_word = [&](int w) {
-            const int tx = code & 1023, ty = (code >> 10) & 1023, tz = code >> 20;
-            return __ldg(masks + tx * W + w) & __ldg(masks + (kGridTri + ty) * W + w) &
-                   __ldg(masks + (2 * kGridTri + tz) * W + w);
-        };
-        // Compact the surviving (primitive, link) pairs, link-major: lane g counts
-        // link g's candidates, an exclusive warp scan gives each link its offset,
-        // and every lane writes its own link's pairs in primitive order.
-        int cnt = 0;
-        if (code >= 0)
-            for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
-        int off = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(kFull, off, o);
-            if (lane >= o) off += y;
-        }
-        const int C = __shfl_sync(kFull, off, 31);
-        off -= cnt;
-
-        bool collide = false, undecided = false;
-        WalkStats st;
-        // Pair list entries [seg0, seg1): lane g writes link g's candidates that
-        // fall in the range.
-        auto write_seg = [&](int seg0, int seg1) {
-            if (cnt > 0 && off < seg1 && off + cnt > seg0) {
-                int idx = off;
-                for (int w = 0; w < W && idx < seg1; ++w) {
-                    uint64_t m = mask_word(w);
-                    while (m && idx < seg1) {
-                        const int b = __ffsll((long long)m) - 1;
-                        if (idx >= seg0) pairs[idx - seg0] = (uint16_t)(((w * 64 + b) << GB) | lane);
-                        ++idx;
-                        m &= m - 1;
-                    }
-                }
-            }
-            __syncwarp();
-        };
-        auto walk_seg = [&](int Cs) {
-            const int n = P.steps[e];
-            const size_t row0 = (size_t)P.offs[e];
-            // Learned order: rank the edge's 4 n segments by their MLP score
-            // (descending, ties by index; NaN scores last).
-            const int nseg = 4 * n;
-            const int seg_row = MODE == 2 ? P.q_rows[(size_t)cta * P.edges_per_cta + slot] : -1;
-            const bool learned = MODE == 2 && seg_row >= 0 && nseg <= kMaxSegments;
-            if (learned) {
-                float v0 = lane < nseg ? P.logits[seg_row + lane] : -INFINITY;
-                float v1 = lane + 32 < nseg ? P.logits[seg_row + lane + 32] : -INFINITY;
-                v0 = isnan(v0) ? -INFINITY : v0;
-                v1 = isnan(v1) ? -INFINITY : v1;
-                int rank0 = 0, rank1 = 0;
-                for (int i = 0; i < nseg; ++i) {
-                    const float vi = __shfl_sync(kFull, i < 32 ? v0 : v1, i & 31);
-                    rank0 += (vi > v0 || (vi == v0 && i < lane)) ? 1 : 0;
-                    rank1 += (vi > v1 || (vi == v1 && i < lane + 32)) ? 1 : 0;
-                }
-                if (lane < nseg) s_perm[warp][rank0] = (uint8_t)lane;
-                if (lane + 32 < nseg) s_perm[warp][rank1] = (uint8_t)(lane + 32);
-                __syncwarp();
-            }
-            collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np,
-                                          learned ? s_perm[warp] : nullptr, P.queue_min_items, GL, undecided, st);
-            __syncwarp();  // every lane is done with this segment's pairs
-        };
-        // Robots whose leaves all lie inside their bounds have a small walk: a
-        // separate copy for the usual single-segment case keeps the segment
-        // bookkeeping out of it.  The overhang-aware walk stays in one copy.
-        bool single = false;
-        if constexpr (!has_overhang<M>()) single = C > 0 && C <= K;
-        if (single) {
-            write_seg(0, C);
-            walk_seg(C);
-        } else {
-            for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
-                const int seg1 = min(C, seg0 + K);
-                write_seg(seg0, seg1);
-                walk_seg(seg1 - seg0);
-            }
-        }
-        if (MODE == 1 && undecided) {
-            if (lane == 0) {
-                const int n = P.steps[e];
-                const int qi = atomicAdd(P.q_count + cta, 1);
-                int ro = -1;
-                if (4 * n <= kMaxSegments) {
-                    ro = atomicAdd(P.row_count, 4 * n);
-                    if (ro > P.row_cap - 4 * n) ro = -1;
-                }
-                P.q_edges[(size_t)cta * P.edges_per_cta + qi] = e;
-                P.q_rows[(size_t)cta * P.edges_per_cta + qi] = ro;
-            }
-            continue;
-        }
-        if (lane == 0) {
-            *out = collide ? 1 : 0;
-            if (P.counters) {
-                atomicAdd(P.counters + 0, 1ull);
-                atomicAdd(P.counters + 1, (unsigned long long)C);
-                atomicAdd(P.counters + 2, st.chunks);
-                atomicAdd(P.counters + 3, st.gates);
-                atomicAdd(P.counters + 4, st.leaf);
-                atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
-            }
-        }
-    }
+    for (int slot = warp; slot < n_slots; slot += WARPS)
+        check_pair<M, MODE>(P, env, e_begin + slot, -1, prim, masks, np, W, pairs, nullptr, GL);
 }
 
-__device__ __forceinline__ int tile_slots(const CheckParams& P, int env, int tile, int mode) {
-    if (mode == 2) return P.q_count[tile * P.num_envs + env];
+__device__ __forceinline__ int tile_slots(const CheckParams& P, int tile) {
     const int e_begin = tile * P.edges_per_cta;
     return min(P.edges_per_cta, P.num_edges - e_begin);
 }
@@ -677,9 +697,8 @@ template <class M, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
-    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
     const int env = blockIdx.x, tile = blockIdx.y;
-    const int n_slots = tile_slots(P, env, tile, MODE);
+    const int n_slots = tile_slots(P, tile);
     if (n_slots <= 0) return;
     const float4 h0 = P.env_hdr[2 * env + 0];
     const float4 h1 = P.env_hdr[2 * env + 1];
@@ -697,7 +716,7 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
             return;
         }
     }
-    check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, s_perm, h0, h1);
+    check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, h0, h1);
 }
 
 // Persistent: a grid sized to the resident capacity pulls environment-major
@@ -709,7 +728,6 @@ template <class M, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_persistent_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
-    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
     __shared__ int s_item;
     const int tiles = (P.num_edges + P.edges_per_cta - 1) / P.edges_per_cta;
     const long long items = (long long)P.num_envs * tiles;
@@ -729,7 +747,7 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
         bool failed = false;
         for (int item = first; item < first + kItemsPerGrab && item < items; ++item) {
             const int env = item / tiles, tile = item - (item / tiles) * tiles;
-            const int n_slots = tile_slots(P, env, tile, MODE);
+            const int n_slots = tile_slots(P, tile);
             if (n_slots <= 0) continue;
             const float4 h0 = P.env_hdr[2 * env + 0];
             const float4 h1 = P.env_hdr[2 * env + 1];
@@ -749,10 +767,52 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
                 }
                 staged = env;
             }
-            check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, s_perm, h0, h1);
+            check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, h0, h1);
         }
         if (failed) break;
         __syncthreads();
+    }
+}
+
+// Learned order, phase 3: every warp pulls queued pairs from finish_counter,
+// one at a time (queued pairs differ in length by two orders of magnitude),
+// and walks each with its segments in descending MLP score.  Consecutive pulls
+// belong to different environments, so the primitive records are read from
+// global memory (L1/L2) rather than staged; shared memory holds the warps'
+// pair lists only.  Compiled for at most 32 resident warps per SM: its walk
+// holds 64-bit record pointers and the segment permutation, and spills in the
+// plain check kernel's tighter register budget.
+template <class M, int WARPS>
+constexpr int finish_min_ctas() {
+    return (M::check_warps_per_sm < 32 ? M::check_warps_per_sm : 32) / WARPS;
+}
+
+template <class M, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finish_kernel(CheckParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long queued = (long long)(*P.q_head >> 32);
+    const int total = (int)min(queued, (long long)P.q_cap);
+    uint16_t* pairs = reinterpret_cast<uint16_t*>(smem) + (size_t)warp * P.pairs_per_warp;
+    const GroupLanes GL = group_lanes<M>();
+    for (;;) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(P.finish_counter, 1);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= total) break;
+        const int ro = P.q_rows[i];
+        if (ro < 0) continue;  // the probe walked this pair on
+        const int2 pe = P.q_pairs[i];
+        const int env = pe.y;
+        const float4 h0 = P.env_hdr[2 * env + 0];
+        const float4 h1 = P.env_hdr[2 * env + 1];
+        const uint32_t shape = __float_as_uint(h1.w);
+        const int np = (int)(shape & 0xffffu);
+        const int W = (int)(shape >> 16);
+        const float4* prim = P.blobs + __float_as_uint(h0.w);
+        const uint64_t* masks = reinterpret_cast<const uint64_t*>(prim + (size_t)np * kPrimF4);
+        check_pair<M, 2>(P, env, pe.x, ro, prim, masks, np, W, pairs, s_perm[warp], GL);
     }
 }
 
@@ -782,18 +842,19 @@ __device__ __forceinline__ void write_features(const float* q, const float* code
 }
 
 // Features of every queued pair's segments: row ro + j is segment j scored at
-// its middle sample k = 8 j + 4.  One warp per queued pair.
+// its middle sample k = 8 j + 4.  One warp per queue entry, grid-strided.
 template <class M>
 __global__ void queue_features_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
                                       uint16_t* __restrict__ x) {
-    const int cta = blockIdx.x;
-    const int env = cta % P.num_envs;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nq = P.q_count[cta];
-    for (int slot = warp; slot < nq; slot += blockDim.x >> 5) {
-        const int ro = P.q_rows[(size_t)cta * P.edges_per_cta + slot];
+    const int lane = threadIdx.x & 31;
+    const long long queued = (long long)(*P.q_head >> 32);
+    const int total = (int)min(queued, (long long)P.q_cap);
+    const int stride = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < total; i += stride) {
+        const int ro = P.q_rows[i];
         if (ro < 0) continue;
-        const int e = P.q_edges[(size_t)cta * P.edges_per_cta + slot];
+        const int2 pe = P.q_pairs[i];
+        const int e = pe.x, env = pe.y;
         const int n = P.steps[e];
         float s[M::dof], t[M::dof], q[M::dof];
 #pragma unroll
@@ -946,7 +1007,7 @@ __global__ void __launch_bounds__(WARPS * 32) check_records_kernel(RecordsParams
         WalkStats st;
         if (C > 0)
             collide = walk_pairs<M, 0>(P.table, (size_t)P.offs[e], P.steps[e], C, pairs, prim, np, nullptr, 0,
-                                       GL, undecided, st);
+                                       GL, undecided, st, [] { return false; });
         __syncwarp();
         if (lane == 0) *out = collide ? 1 : 0;
     }
@@ -992,11 +1053,30 @@ cudaError_t launch_check_wm(CheckParams P, int E, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// Learned order, phase 3: a grid of the resident capacity; the queue length
+// is read on the device.
+template <class M, int W>
+cudaError_t launch_finish_w(CheckParams P, cudaStream_t st) {
+    P.pairs_per_warp = std::min((P.max_prims * M::num_env_groups + 7) & ~7, kPairCap);
+    const size_t smem = (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
+    cudaError_t err = cudaFuncSetAttribute(finish_kernel<M, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finish_kernel<M, W>, W * 32, smem);
+    if (err != cudaSuccess) return err;
+    err = cudaMemsetAsync(P.finish_counter, 0, sizeof(int), st);
+    if (err != cudaSuccess) return err;
+    finish_kernel<M, W><<<std::max(per_sm, 1) * std::max(sms, 1), W * 32, smem, st>>>(P);
+    return cudaGetLastError();
+}
+
 template <class M, int W>
 cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st, int mode) {
     switch (mode) {
         case 1: return launch_check_wm<M, W, 1>(P, E, st);
-        case 2: return launch_check_wm<M, W, 2>(P, E, st);
+        case 2: return launch_finish_w<M, W>(P, st);
         default: return launch_check_wm<M, W, 0>(P, E, st);
     }
 }
