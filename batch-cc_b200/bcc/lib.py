@@ -38,7 +38,7 @@ class BccError(RuntimeError):
 
 class BccOpts(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int32), ("use_graph", ctypes.c_int32),
-                ("tile_override", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("tile_override", ctypes.c_int32), ("learned_row_cap", ctypes.c_int32)]
 
 
 _lib = None
@@ -100,11 +100,12 @@ def exported_symbols():
             "bcc_set_profiling", "bcc_stage_times", "bcc_measure_fp32_peak", "bcc_work_counters"]
 
 
-def make_opts(order="plain", use_graph=False, tile=0):
+def make_opts(order="plain", use_graph=False, tile=0, row_cap=0):
     o = BccOpts()
     o.order = ORDERS[order]
     o.use_graph = int(bool(use_graph))
     o.tile_override = int(tile)
+    o.learned_row_cap = int(row_cap)
     return o
 
 
@@ -136,13 +137,14 @@ class Checker:
         self._raise(lib().bcc_upload_envs(self._h, ctypes.byref(soa)))
         self.num_envs = envset.num_envs
 
-    def check(self, edges, resolution=32, robot="panda", order="plain", out=None, tile=0, graph=False):
-        """Host API: edges float32 [E, 2, dof] -> verdicts uint8 [E, num_envs]."""
+    def check(self, edges, resolution=32, robot="panda", order="plain", out=None, tile=0, graph=False, row_cap=0):
+        """Host API: edges float32 [E, 2, dof] -> verdicts uint8 [E, num_envs].  row_cap > 0 bounds the
+        learned order's MLP rows per check."""
         edges = np.ascontiguousarray(edges, np.float32)
         E = edges.shape[0]
         if out is None:
             out = np.zeros((E, self.num_envs), np.uint8)
-        opts = make_opts(order, use_graph=graph, tile=tile)
+        opts = make_opts(order, use_graph=graph, tile=tile, row_cap=row_cap)
         st = lib().bcc_check(self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                              E, resolution, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
                              ctypes.byref(opts))
@@ -242,9 +244,9 @@ class Checker:
         return dict(zip(self.CONFIG, list(c)))
 
     def check_device(self, d_edges_ptr, num_edges, d_results_ptr, resolution=32, robot="panda",
-                     order="plain", stream=0, tile=0, graph=False):
+                     order="plain", stream=0, tile=0, graph=False, row_cap=0):
         """Device API: raw device pointers (e.g. torch tensors' data_ptr()), stream-ordered."""
-        opts = make_opts(order, use_graph=graph, tile=tile)
+        opts = make_opts(order, use_graph=graph, tile=tile, row_cap=row_cap)
         st = lib().bcc_check_device(self._h, _rid(robot), ctypes.c_void_p(d_edges_ptr), num_edges,
                                     resolution, ctypes.c_void_p(d_results_ptr), ctypes.byref(opts),
                                     ctypes.c_void_p(stream))

@@ -226,9 +226,9 @@ constexpr int kLearnedRowCap = 16 << 20;  // MLP rows per learned check (1.5 GB 
 // queued with MLP rows for their segments; (2) segment features and tcgen05
 // MLP scores; (3) the queued pairs walked in descending segment score.
 // Buffers are sized here, outside any stream capture.
-bcc_status prepare_learned(bcc_ctx* ctx, bcc::PipelineArgs& a) {
+bcc_status prepare_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, int row_cap) {
     const long long cap_ll = (long long)a.num_envs * (a.total_rows / bcc::kSegment) + 64;
-    const int cap = (int)std::min<long long>(cap_ll, kLearnedRowCap);
+    const int cap = (int)std::min<long long>(cap_ll, row_cap > 0 ? std::min(row_cap, kLearnedRowCap) : kLearnedRowCap);
     // A queued pair takes at least 4 rows; the probe stops queueing once the
     // rows are spent, so the queue needs cap / 4 entries plus the pairs that
     // were in flight at that moment (the kernel checks the capacity anyway).
@@ -297,7 +297,9 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
             return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned order needs MLP parameters (bcc_mlp_train or bcc_mlp_set_params)");
         s = ensure_env_code(ctx, st);
         if (s != BCC_OK) return s;
-        s = prepare_learned(ctx, a);
+        if (opts->learned_row_cap < 0)
+            return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned_row_cap must be >= 0");
+        s = prepare_learned(ctx, a, opts->learned_row_cap);
         if (s != BCC_OK) return s;
     }
     const bool graph = opts && opts->use_graph && !ctx->counting && !(opts->tile_override > 0);
@@ -307,6 +309,7 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
     bcc::GraphCache& G = ctx->graph[learned ? 1 : 0];
     const bool hit = G.exec && G.edges == d_edges && G.results == d_results && G.num_edges == E &&
                      G.resolution == resolution && G.total_rows == a.total_rows && G.robot == (int)robot &&
+                     G.row_cap == a.row_cap &&
                      G.env_version == ctx->env_version && same_tune(G.tune, ctx->tune);
     if (!hit) {
         if (G.exec) {
@@ -335,6 +338,7 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
         G.num_edges = E;
         G.resolution = resolution;
         G.total_rows = a.total_rows;
+        G.row_cap = a.row_cap;
         G.robot = (int)robot;
         G.env_version = ctx->env_version;
         G.tune = ctx->tune;

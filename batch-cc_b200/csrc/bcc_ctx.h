@@ -58,7 +58,7 @@ struct GraphCache {
     const void* edges = nullptr;
     void* results = nullptr;
     cudaStream_t stream = nullptr;
-    int num_edges = -1, resolution = -1, total_rows = -1, order = -1, robot = -1;
+    int num_edges = -1, resolution = -1, total_rows = -1, order = -1, robot = -1, row_cap = -1;
     long long env_version = -1;
     Tune tune;
     ~GraphCache() {

@@ -81,8 +81,9 @@ def parse():
                    help="profiling run: only `--warmup` + `--steps` eager checks in this order (launch config "
                         "--profile-launch, MLP at its seeded initialisation), no training, tuning or baselines")
     p.add_argument("--profile-launch", default="128,4,0",
-                   help="edges per CTA, warps per CTA, persistent (0/1) of a profiling run; the default is the "
-                        "configuration the autotuner picks for the plain order of the uneven workload")
+                   help="edges per CTA, warps per CTA, persistent (0/1) and optionally the learned-order queue "
+                        "threshold of a profiling run; the default is the configuration the autotuner picks for "
+                        "the plain order of the uneven workload")
     p.add_argument("--envs", type=int, default=None, help="smaller case for profiling")
     p.add_argument("--edges", type=int, default=None, help="smaller case for profiling")
     return p.parse_args()
@@ -349,8 +350,11 @@ def run_profile(args, local):
     chk.upload(envs)
     if args.profile_order == "learned":
         chk.mlp_set_params(mlp.init_params(1000))
-    tile, warps, persistent = (int(v) for v in args.profile_launch.split(","))
+    launch = [int(v) for v in args.profile_launch.split(",")]
+    tile, warps, persistent = launch[:3]
     chk.set_launch_config(edges_per_cta=tile, warps=warps, persistent=persistent)
+    if len(launch) > 3:
+        chk.set_launch_config(queue_min_items=launch[3])
     for _ in range(args.warmup + args.steps):
         chk.check(edges, order=args.profile_order, robot=robot)
     torch.cuda.synchronize()

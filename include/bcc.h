@@ -81,7 +81,8 @@ typedef struct bcc_opts {
     int32_t order;         /* bcc_order */
     int32_t use_graph;     /* 1: replay a captured CUDA graph of the launch sequence */
     int32_t tile_override; /* 0: autotuned tile; >0: force a tile id (tuning/tests) */
-    int32_t reserved;
+    int32_t learned_row_cap; /* learned order: 0 = default budget of MLP rows (segments scored) per
+                              * check, >0 = at most this many; pairs beyond it keep the plain order */
 } bcc_opts;
 
 typedef struct bcc_ctx bcc_ctx;

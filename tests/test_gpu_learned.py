@@ -59,3 +59,34 @@ def test_trained_network_saves_work(checker, trained):
     checker.set_profiling(False)
     assert work["trained"]["colliding"] == work["untrained"]["colliding"]
     assert work["trained"]["chunks"] <= work["untrained"]["chunks"], work
+
+
+@pytest.mark.parametrize("row_cap", [3, 4, 64, 2000])
+@pytest.mark.parametrize("graph", [False, True])
+def test_row_budget_keeps_verdicts(checker, trained, row_cap, graph):
+    """A row budget smaller than the queue needs: pairs that find it spent (or
+    whose segments would not fit) are walked on in plain order by the probe,
+    the rest are scored and finished; verdicts stay the plain order's.  A budget
+    below 4 rows queues nothing."""
+    checker.mlp_set_params(trained["params"])
+    envs = workload.gen_envs("stress", 24, seed=41)
+    edges = workload.gen_edges("stress", 400, seed=41)
+    checker.upload(envs)
+    plain = checker.check(edges, order="plain")
+    for _ in range(2):  # the second call replays the captured graph when graph=True
+        learned = checker.check(edges, order="learned", graph=graph, row_cap=row_cap)
+        assert np.array_equal(plain, learned)
+        rows = checker.last_learned_rows()
+        assert 0 <= rows <= row_cap
+        if row_cap < 4:
+            assert rows == 0
+    # the default budget scores more rows than any of the small ones
+    checker.check(edges, order="learned")
+    assert checker.last_learned_rows() > min(row_cap, 64)
+
+
+def test_negative_row_budget_is_rejected(checker, trained):
+    checker.mlp_set_params(trained["params"])
+    checker.upload(workload.gen_envs("stress", 4, seed=42))
+    with pytest.raises(Exception, match="learned_row_cap"):
+        checker.check(workload.gen_edges("stress", 10, seed=42), order="learned", row_cap=-1)
