@@ -79,6 +79,8 @@ def lib():
                                        ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
         L.bcc_last_learned_rows.argtypes = [vp]
         L.bcc_last_learned_rows.restype = ctypes.c_int64
+        L.bcc_last_learned_pairs.argtypes = [vp]
+        L.bcc_last_learned_pairs.restype = ctypes.c_int64
         L.bcc_get_launch_config.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
         L.bcc_set_launch_config.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
         L.bcc_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32, ctypes.c_int32,
@@ -222,6 +224,9 @@ class Checker:
 
     def last_learned_rows(self):
         return int(lib().bcc_last_learned_rows(self._h))
+
+    def last_learned_pairs(self):
+        return int(lib().bcc_last_learned_pairs(self._h))
 
     CONFIG = ("edges_per_cta", "warps", "persistent", "queue_min_items")
 

@@ -94,8 +94,9 @@ struct bcc_ctx {
     bcc::DevBuf env_code;    // [num_envs][32] environment encodings
     bool env_code_ready = false;
     bcc::DevBuf q_head, q_pairs, q_rows;   // learned-order queue of undecided pairs
-    const int* learned_rows_dev = nullptr; // device row count of the last learned check
+    const int* learned_rows_dev = nullptr; // queue head of the last learned check (entries << 32 | rows)
     int learned_row_cap = 0;
+    int learned_q_cap = 0;
     bcc::Tune tune;                        // launch configuration (autotuned or default)
     bcc::DevBuf work_counter;              // persistent-kernel work queue head
     long long env_version = 0;             // bumped by every upload (graph cache key)

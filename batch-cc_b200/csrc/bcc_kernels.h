@@ -84,7 +84,7 @@ struct PipelineArgs {
     int* error_flag;
     cudaEvent_t* stage_events;  // null, or 6 events bracketing the 5 stages
     unsigned long long* counters;
-    int mode;                // 0 plain, 1 probe (first chunk, queue the rest), 2 finish (learned order)
+    int mode;                // 0 plain, 1 probe (rank 0, queue the rest), 2 finish (learned order)
     unsigned long long* q_head;
     int2* q_pairs;
     int* q_rows;

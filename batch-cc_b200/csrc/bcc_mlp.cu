@@ -133,6 +133,9 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
                        int* __restrict__ err) {
     // rows_dev (optional): the row count produced on the device, capped by rows.
     if (rows_dev) rows = min(rows, *rows_dev);
+    // The grid is sized for the host's row bound; CTAs without a tile of the
+    // device count leave before loading the weights.
+    if ((long long)blockIdx.x * kFwdGroups * 128 >= (long long)rows) return;
     extern __shared__ __align__(1024) uint8_t sm[];
     const int t = threadIdx.x, warp = t >> 5, grp = t >> 7, gt = t & 127;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmBar) + grp;

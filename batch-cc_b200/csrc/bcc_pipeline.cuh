@@ -358,31 +358,51 @@ __device__ __forceinline__ GroupLanes group_lanes() {
 
 // Whole warp: walk (sample rank, pair) items 32 at a time in check order --
 // plain reference order, or with `perm` the edge's segments in learned order --
-// and return whether some item collides.  MODE 1 (probe): after the first
-// chunk, when at least queue_min_items remain, the whole warp calls queue();
-// if that queues the pair, the walk stops with `undecided` set, otherwise it
-// goes on in plain order.
+// and return whether some item collides.  MODE 1 (probe): after the chunk that
+// completes rank 0, when at least queue_min_items remain, the whole warp calls
+// queue(); if that queues the pair, the walk stops with `undecided` set,
+// otherwise it goes on in plain order.
 // Each chunk tests the bounds (one per item); the leaf work of the items whose
 // bound hit is then flattened over the warp (item j owns leaf slots
 // [incl_j - cnt_j, incl_j)) and the warp stops at the first step with a hit.
+// MODE 2 (finish): the CTA's warps split the pair -- this warp walks chunks
+// chunk0, chunk0 + stride, ... and all stop once one of them sets *stop.
 template <class M, int MODE, class Queue>
 __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, size_t row0, int n, int C,
                                            const uint16_t* pairs, const float4* prim, int np, const uint8_t* perm,
                                            int queue_min_items, const GroupLanes& GL, bool& undecided,
-                                           WalkStats& st, Queue&& queue) {
+                                           WalkStats& st, Queue&& queue, int chunk0 = 0, int stride = 1,
+                                           volatile int* stop = nullptr) {
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
     constexpr bool kOver = has_overhang<M>();
     const int lane = threadIdx.x & 31;
     const int total = kLanes * n * C;
-    // a / C for a <= 32 and 1 <= C <= kPairCap: floor((a + 0.5) / C) in FP32 is
-    // exact (the quotient stays >= 1 / 2048 away from an integer), and cheaper
-    // than an integer division by a runtime divisor.
-    const float inv_c = __frcp_rn((float)C);
-    const int dr = (int)(32.5f * inv_c), dc = 32 - dr * C;
-    int r = (int)(((float)lane + 0.5f) * inv_c), c = lane - r * C;
+    int dr, dc, r, c, w_begin = 0, w_step = 32;
+    if constexpr (MODE == 2) {
+        w_begin = 32 * chunk0;
+        w_step = 32 * stride;
+        dr = w_step / C;
+        dc = w_step - dr * C;
+        r = (w_begin + lane) / C;
+        c = w_begin + lane - r * C;
+    } else {
+        // a / C for a <= 32 and 1 <= C <= kPairCap: floor((a + 0.5) / C) in FP32 is
+        // exact (the quotient stays >= 1 / 2048 away from an integer), and cheaper
+        // than an integer division by a runtime divisor.
+        const float inv_c = __frcp_rn((float)C);
+        dr = (int)(32.5f * inv_c);
+        dc = 32 - dr * C;
+        r = (int)(((float)lane + 0.5f) * inv_c);
+        c = lane - r * C;
+    }
     bool collide = false;
-    for (int w0 = 0; w0 < total; w0 += 32) {
+    for (int w0 = w_begin; w0 < total; w0 += w_step) {
+        if constexpr (MODE == 2) {  // another warp of the CTA found a hit
+            int s = 0;
+            if (lane == 0) s = *stop;
+            if (__shfl_sync(kFull, s, 0)) break;
+        }
         bool gate = false;
         int g = 0, p = 0, k = 0, cnt = 0, first = 0;
         if constexpr (!kOver) {
@@ -489,9 +509,11 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
             }
             if (collide) break;
         }
-        // Probe: after the first chunk, queue the pair for the learned order
-        // only when much work remains; small remainders finish in plain order.
-        if (MODE == 1 && w0 == 0 && total - 32 >= queue_min_items && queue()) {
+        // Probe: once the chunk that completes rank 0 (the edge's first sample
+        // against every candidate, where most colliding pairs collide) is
+        // walked, queue the pair for the learned order only when much work
+        // remains; small remainders finish in plain order.
+        if (MODE == 1 && w0 == (((C - 1) >> 5) << 5) && total - (w0 + 32) >= queue_min_items && queue()) {
             undecided = true;
             break;
         }
@@ -501,6 +523,9 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
             c -= C;
             ++r;
         }
+    }
+    if constexpr (MODE == 2) {
+        if (collide && lane == 0) *stop = 1;
     }
     return collide;
 }
@@ -528,7 +553,7 @@ __device__ __forceinline__ int queue_pair(const CheckParams& P, int e, int env, 
 
 // One (environment, edge) pair, whole warp: cull, pair-list compaction and the
 // walk.  MODE 0: plain order, full walk.  MODE 1 (learned pipeline, phase 1):
-// plain order; a pair still undecided after its first 32-item chunk may be
+// plain order; a pair still undecided once rank 0 (its first sample) is walked may be
 // queued (with MLP rows for its segments) instead of getting a verdict.  MODE 2
 // (phase 3): a queued pair (first MLP row seg_row) walked in descending
 // segment score.  `prim` holds the environment's records (shared or global
@@ -536,7 +561,8 @@ __device__ __forceinline__ int queue_pair(const CheckParams& P, int e, int env, 
 template <class M, int MODE>
 __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e, int seg_row, const float4* prim,
                                            const uint64_t* __restrict__ masks, int np, int W, uint16_t* pairs,
-                                           uint8_t* perm_buf, const GroupLanes& GL) {
+                                           uint8_t* perm_buf, const GroupLanes& GL, int chunk0 = 0, int stride = 1,
+                                           volatile int* stop = nullptr) {
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
     const int lane = threadIdx.x & 31;
@@ -544,7 +570,10 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
     uint8_t* out = P.results + (size_t)e * P.num_envs + env;
     const int self = P.edge_self[e];
     if (np == 0 || self) {  // a self-colliding sample collides in every environment
-        if (lane == 0) *out = self ? 1 : 0;
+        if (lane == 0) {
+            *out = self ? 1 : 0;
+            if (MODE == 2 && self) *stop = 1;  // the finish kernel writes s_hit as the verdict
+        }
         return;
     }
     // Cull: lane g < G takes link g's slab ranges on the set's grid (computed
@@ -619,7 +648,7 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
             __syncwarp();
         }
         collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np, learned ? perm_buf : nullptr,
-                                      P.queue_min_items, GL, undecided, st, queue);
+                                      P.queue_min_items, GL, undecided, st, queue, chunk0, stride, stop);
         __syncwarp();  // every lane is done with this segment's pairs
     };
     // Robots whose leaves all lie inside their bounds have a small walk: a
@@ -638,6 +667,15 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
         }
     }
     if (MODE == 1 && undecided) return;  // queued: the finish pass writes the verdict
+    if (MODE == 2) {  // the CTA's warps split the pair: the finish kernel writes the verdict
+        if (lane == 0 && P.counters) {
+            if (chunk0 == 0) atomicAdd(P.counters + 1, (unsigned long long)C);
+            atomicAdd(P.counters + 2, st.chunks);
+            atomicAdd(P.counters + 3, st.gates);
+            atomicAdd(P.counters + 4, st.leaf);
+        }
+        return;
+    }
     if (lane == 0) {
         *out = collide ? 1 : 0;
         if (P.counters) {
@@ -774,14 +812,17 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
     }
 }
 
-// Learned order, phase 3: every warp pulls queued pairs from finish_counter,
-// one at a time (queued pairs differ in length by two orders of magnitude),
-// and walks each with its segments in descending MLP score.  Consecutive pulls
+// Learned order, phase 3: each CTA pulls queued pairs from finish_counter, one
+// at a time, and its warps split each pair's walk (warp w takes chunks w,
+// w + WARPS, ... of the learned order; a hit in any stops all): the queued
+// pairs are the longest walks of the check, and one warp per pair would leave
+// the slowest single walk as the kernel's critical path.  The verdict is the
+// OR over all items, so the split changes no verdict.  Consecutive pulls
 // belong to different environments, so the primitive records are read from
 // global memory (L1/L2) rather than staged; shared memory holds the warps'
-// pair lists only.  Compiled for at most 32 resident warps per SM: its walk
-// holds 64-bit record pointers and the segment permutation, and spills in the
-// plain check kernel's tighter register budget.
+// pair lists only (each warp compacts its own copy).  Compiled for at most 32
+// resident warps per SM: its walk holds 64-bit record pointers and the segment
+// permutation, and spills in the plain check kernel's tighter register budget.
 template <class M, int WARPS>
 constexpr int finish_min_ctas() {
     return (M::check_warps_per_sm < 32 ? M::check_warps_per_sm : 32) / WARPS;
@@ -791,28 +832,42 @@ template <class M, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finish_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint8_t s_perm[WARPS][kMaxSegments];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int s_item;
+    __shared__ volatile int s_hit;
+    const int warp = threadIdx.x >> 5;
     const long long queued = (long long)(*P.q_head >> 32);
     const int total = (int)min(queued, (long long)P.q_cap);
     uint16_t* pairs = reinterpret_cast<uint16_t*>(smem) + (size_t)warp * P.pairs_per_warp;
     const GroupLanes GL = group_lanes<M>();
     for (;;) {
-        int i = 0;
-        if (lane == 0) i = atomicAdd(P.finish_counter, 1);
-        i = __shfl_sync(kFull, i, 0);
-        if (i >= total) break;
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(P.finish_counter, 1);
+            s_hit = 0;
+        }
+        __syncthreads();
+        const int i = s_item;
+        if (i >= total) break;  // CTA-uniform
         const int ro = P.q_rows[i];
-        if (ro < 0) continue;  // the probe walked this pair on
-        const int2 pe = P.q_pairs[i];
-        const int env = pe.y;
-        const float4 h0 = P.env_hdr[2 * env + 0];
-        const float4 h1 = P.env_hdr[2 * env + 1];
-        const uint32_t shape = __float_as_uint(h1.w);
-        const int np = (int)(shape & 0xffffu);
-        const int W = (int)(shape >> 16);
-        const float4* prim = P.blobs + __float_as_uint(h0.w);
-        const uint64_t* masks = reinterpret_cast<const uint64_t*>(prim + (size_t)np * kPrimF4);
-        check_pair<M, 2>(P, env, pe.x, ro, prim, masks, np, W, pairs, s_perm[warp], GL);
+        const int2 pe = ro >= 0 ? P.q_pairs[i] : make_int2(0, 0);
+        if (ro >= 0) {  // ro < 0: the probe walked this pair on
+            const int env = pe.y;
+            const float4 h0 = P.env_hdr[2 * env + 0];
+            const float4 h1 = P.env_hdr[2 * env + 1];
+            const uint32_t shape = __float_as_uint(h1.w);
+            const int np = (int)(shape & 0xffffu);
+            const int W = (int)(shape >> 16);
+            const float4* prim = P.blobs + __float_as_uint(h0.w);
+            const uint64_t* masks = reinterpret_cast<const uint64_t*>(prim + (size_t)np * kPrimF4);
+            check_pair<M, 2>(P, env, pe.x, ro, prim, masks, np, W, pairs, s_perm[warp], GL, warp, WARPS, &s_hit);
+        }
+        __syncthreads();  // every warp is done with this pair (and with s_item)
+        if (threadIdx.x == 0 && ro >= 0) {
+            P.results[(size_t)pe.x * P.num_envs + pe.y] = s_hit ? 1 : 0;
+            if (P.counters) {
+                atomicAdd(P.counters + 0, 1ull);
+                atomicAdd(P.counters + 5, s_hit ? 1ull : 0ull);
+            }
+        }
     }
 }
 
@@ -842,15 +897,20 @@ __device__ __forceinline__ void write_features(const float* q, const float* code
 }
 
 // Features of every queued pair's segments: row ro + j is segment j scored at
-// its middle sample k = 8 j + 4.  One warp per queue entry, grid-strided.
+// its middle sample k = 8 j + 4.  Eight lanes per queue entry (four entries per
+// warp in flight, grid-strided), each lane one segment at a time: the loads
+// of an entry form a dependent chain, so several entries per warp hide it.
+constexpr int kFeatureLanes = 8;
+
 template <class M>
 __global__ void queue_features_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
                                       uint16_t* __restrict__ x) {
-    const int lane = threadIdx.x & 31;
+    const int sl = threadIdx.x & (kFeatureLanes - 1);
     const long long queued = (long long)(*P.q_head >> 32);
     const int total = (int)min(queued, (long long)P.q_cap);
-    const int stride = gridDim.x * (blockDim.x >> 5);
-    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < total; i += stride) {
+    const int per_cta = blockDim.x / kFeatureLanes;
+    const int stride = gridDim.x * per_cta;
+    for (int i = blockIdx.x * per_cta + threadIdx.x / kFeatureLanes; i < total; i += stride) {
         const int ro = P.q_rows[i];
         if (ro < 0) continue;
         const int2 pe = P.q_pairs[i];
@@ -862,7 +922,7 @@ __global__ void queue_features_kernel(CheckParams P, const float* __restrict__ e
             s[j] = edges[(size_t)e * 2 * M::dof + j];
             t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
         }
-        for (int seg = lane; seg < 4 * n; seg += 32) {
+        for (int seg = sl; seg < 4 * n; seg += kFeatureLanes) {
             edge_sample<M::dof>(s, t, n, seg * kSegment + kSegment / 2, q);
             write_features<M>(q, code + (size_t)env * kEnvCode, x + (size_t)(ro + seg) * kMlpIn);
         }

@@ -387,7 +387,7 @@ def run_ours(args, world, rank, local, dist):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
     # Autotuned launch configuration per order (untimed), on the first edges.
-    tuned = {o: chk.autotune(edges[:min(E, 2000)], order=o, robot=robot) for o in ("plain", "learned")}
+    tuned = {o: chk.autotune(edges[:min(E, 10000)], order=o, robot=robot) for o in ("plain", "learned")}
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -424,6 +424,7 @@ def run_ours(args, world, rank, local, dist):
     chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream, robot=robot)
     torch.cuda.synchronize()
     learned_rows = chk.last_learned_rows()
+    learned_pairs = chk.last_learned_pairs()
 
     # e2e: the public host API (pinned host edges in, verdicts out), per step.
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
@@ -454,7 +455,8 @@ def run_ours(args, world, rank, local, dist):
                            "work_per_pair": work[o]} for o in results},
             "learned_over_plain": ms["plain"] / ms["learned"],
             "verdict_mismatches_learned_vs_plain": mismatch,
-            "proposal": dict(proposal, scored_segments_per_step=learned_rows),
+            "proposal": dict(proposal, scored_segments_per_step=learned_rows, queued_pairs_per_step=learned_pairs,
+                             queued_fraction=learned_pairs / float(N * E)),
             "gpu_launches": (6 + 9) * args.steps,  # plain: 6 launches per step; learned: 9
             "clocks": clk.summary()}
     line["e2e"] = {"value": world * N * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(edges.nbytes),

@@ -214,6 +214,9 @@ bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, i
                             int64_t num_samples, uint64_t seed, float* h_metrics);
 /* MLP rows (segments) scored by the last learned-order check. */
 int64_t bcc_last_learned_rows(const bcc_ctx* ctx);
+/* (environment, edge) pairs the last learned-order check queued for the MLP
+ * order (the others were decided, or walked on, in plain order by the probe). */
+int64_t bcc_last_learned_pairs(const bcc_ctx* ctx);
 /* One Adam step (learning rate lr) on the gradient of the batch. */
 bcc_status bcc_mlp_train_step(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* d_labels, int32_t rows,
                               float lr, float* h_loss);
@@ -228,14 +231,15 @@ bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
  * shared-memory footprint needs it), cfg[2] 1 = persistent kernel pulling
  * (environment, edge tile) work items from an atomic queue, 0 = one CTA per
  * item, cfg[3] learned order: a pair is scored by the MLP only when at least
- * this many (sample, pair) items remain after its first chunk.
+ * this many (sample, pair) items remain once its rank 0 (first sample) is walked.
  */
 bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg);
 bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg);
 /*
  * Autotuner: times candidate configurations (edges per CTA 32..256, 4 or 8
- * warps, persistent or not, and for the learned order the queue threshold) on
- * the given host edges against the uploaded environments and keeps the fastest
+ * warps, persistent or not; for the learned order then the queue threshold
+ * 128..4096 items and the launch shape once more at that threshold) on the
+ * given host edges against the uploaded environments and keeps the fastest
  * in the context; chosen[4] receives it (may be NULL).  order: bcc_order.
  */
 bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,

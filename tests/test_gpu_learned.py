@@ -38,6 +38,8 @@ def test_learned_order_keeps_verdicts(checker, trained, name, nenv, nedge, seed)
     plain = checker.check(edges, order="plain")
     learned = checker.check(edges, order="learned")
     assert checker.last_learned_rows() > 0
+    # every queued pair holds at least its 4 n >= 4 segment rows
+    assert 0 < checker.last_learned_pairs() <= checker.last_learned_rows() // 4
     # Same tests in a different order: identical verdicts.
     assert np.array_equal(plain, learned)
     n_mis, n_adj, bad = orc.adjudicate(envs, edges, learned, orc.check(envs, edges))
