@@ -397,132 +397,144 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
         c = lane - r * C;
     }
     bool collide = false;
-    for (int w0 = w_begin; w0 < total; w0 += w_step) {
-        if constexpr (MODE == 2) {  // another warp of the CTA found a hit
-            int s = 0;
-            if (lane == 0) s = *stop;
-            if (__shfl_sync(kFull, s, 0)) break;
-        }
-        bool gate = false;
-        int g = 0, p = 0, k = 0, cnt = 0, first = 0;
-        if constexpr (!kOver) {
-            // c < C on every lane, also past the last item: the pair is decoded and
-            // its group's leaf range fetched by shuffle on every lane (measured
-            // faster for Panda than lane-indexed constant memory), the table and
-            // the primitive read only for live items.
-            const uint32_t pr = pairs[c];
-            g = (int)(pr & ((1u << GB) - 1u));
-            p = (int)(pr >> GB);
-            first = __shfl_sync(kFull, GL.first, g);
-            const int gcnt = __shfl_sync(kFull, GL.cnt, g);
-            if (w0 + lane < total) {
-                k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
-                float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
-                bs.w += kEnvInflate;
-                gate = sphere_hits_prim(bs, prim + p * kPrimF4);
-                cnt = gate ? gcnt : 0;
+    // Probe: the walk pauses after the chunk that completes rank 0 (the edge's
+    // first sample against every candidate, where most colliding pairs
+    // collide) when at least queue_min_items items remain; the pair is then
+    // queued for the learned order or, if queue() declines, walked on in plain
+    // order.  The pause ends the first pass of the loop, so no chunk pays for
+    // the decision.
+    int w_stop = total;
+    if constexpr (MODE == 1) {
+        const int w_dec = ((C - 1) >> 5) << 5;
+        if (total - (w_dec + 32) >= queue_min_items) w_stop = w_dec + 32;
+    }
+    int w0 = w_begin;
+    for (;;) {
+        for (; w0 < w_stop; w0 += w_step) {
+            if constexpr (MODE == 2) {  // another warp of the CTA found a hit
+                int s = 0;
+                if (lane == 0) s = *stop;
+                if (__shfl_sync(kFull, s, 0)) break;
             }
-        } else {
-            // The overhang-aware walk reads its group fields from constant memory,
-            // which leaves its longer body the registers it needs (measured faster
-            // for Fetch and Baxter).
-            const DevTables<M>& T = tab<M>();
-            if (w0 + lane < total) {
-                k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+            bool gate = false;
+            int g = 0, p = 0, k = 0, cnt = 0, first = 0;
+            if constexpr (!kOver) {
+                // c < C on every lane, also past the last item: the pair is decoded and
+                // its group's leaf range fetched by shuffle on every lane (measured
+                // faster for Panda than lane-indexed constant memory), the table and
+                // the primitive read only for live items.
                 const uint32_t pr = pairs[c];
                 g = (int)(pr & ((1u << GB) - 1u));
                 p = (int)(pr >> GB);
-                float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
-                bs.w += kEnvInflate;
-                float rho;
-                const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
-                const float rr = bs.w + rho;
-                gate = d2 - rr * rr < 0.0f;
-                cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
-                // overhanging leaves (listed first) near a primitive the bound misses
-                if (!gate && T.over_count[g] > 0) {
-                    const float rp = rr + T.cull_pad[g];
-                    if (d2 - rp * rp < 0.0f) cnt = T.over_count[g];
+                first = __shfl_sync(kFull, GL.first, g);
+                const int gcnt = __shfl_sync(kFull, GL.cnt, g);
+                if (w0 + lane < total) {
+                    k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+                    float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
+                    bs.w += kEnvInflate;
+                    gate = sphere_hits_prim(bs, prim + p * kPrimF4);
+                    cnt = gate ? gcnt : 0;
                 }
-            }
-            first = T.leaf_begin[g];
-        }
-        ++st.chunks;
-        if (__any_sync(kFull, cnt > 0)) {
-            ++st.gates;
-            int incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(kFull, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int L = __shfl_sync(kFull, incl, 31);
-            for (int t0 = 0; t0 < L; t0 += 32) {
-                const int t = t0 + lane;
-                // owner j: the first lane whose inclusive count exceeds t
-                int j = 0;
-#pragma unroll
-                for (int step = 16; step; step >>= 1) {
-                    const int v = __shfl_sync(kFull, incl, j + step - 1);
-                    if (v <= t) j += step;
-                }
-                const int j_incl = __shfl_sync(kFull, incl, j);
-                const int j_cnt = __shfl_sync(kFull, cnt, j);
-                const int j_first = __shfl_sync(kFull, first, j);
-                const int j_k = __shfl_sync(kFull, k, j);
-                const int j_p = __shfl_sync(kFull, p, j);
-                bool hit = false;
-                if (t < L) {
-                    const int leaf = j_first + (t - (j_incl - j_cnt));
-                    float4 ls = table[table_index<M>(row0 + (size_t)j_k, G + leaf)];
-                    ls.w += kEnvInflate;
-                    hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
-                }
-                ++st.leaf;
-                if constexpr (kOver) {
-                    const bool j_gate = __shfl_sync(kFull, (int)gate, j) != 0;
-                    if (__any_sync(kFull, hit && j_gate)) {
-                        collide = true;
-                        break;
+            } else {
+                // The overhang-aware walk reads its group fields from constant memory,
+                // which leaves its longer body the registers it needs (measured faster
+                // for Fetch and Baxter).
+                const DevTables<M>& T = tab<M>();
+                if (w0 + lane < total) {
+                    k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+                    const uint32_t pr = pairs[c];
+                    g = (int)(pr & ((1u << GB) - 1u));
+                    p = (int)(pr >> GB);
+                    float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
+                    bs.w += kEnvInflate;
+                    float rho;
+                    const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
+                    const float rr = bs.w + rho;
+                    gate = d2 - rr * rr < 0.0f;
+                    cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
+                    // overhanging leaves (listed first) near a primitive the bound misses
+                    if (!gate && T.over_count[g] > 0) {
+                        const float rp = rr + T.cull_pad[g];
+                        if (d2 - rp * rp < 0.0f) cnt = T.over_count[g];
                     }
-                    // Hits of overhanging leaves whose bound missed this primitive:
-                    // they count once the bound hits some primitive at that sample.
-                    const int j_g = __shfl_sync(kFull, g, j);
-                    uint32_t pend = __ballot_sync(kFull, hit);
-                    while (pend) {
-                        const int u = __ffs(pend) - 1;
-                        const int uk = __shfl_sync(kFull, j_k, u);
-                        const int ug = __shfl_sync(kFull, j_g, u);
-                        if (bound_hits_any<M>(table, row0, uk, ug, prim, np)) {
+                }
+                first = T.leaf_begin[g];
+            }
+            ++st.chunks;
+            if (__any_sync(kFull, cnt > 0)) {
+                ++st.gates;
+                int incl = cnt;
+    #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int L = __shfl_sync(kFull, incl, 31);
+                for (int t0 = 0; t0 < L; t0 += 32) {
+                    const int t = t0 + lane;
+                    // owner j: the first lane whose inclusive count exceeds t
+                    int j = 0;
+    #pragma unroll
+                    for (int step = 16; step; step >>= 1) {
+                        const int v = __shfl_sync(kFull, incl, j + step - 1);
+                        if (v <= t) j += step;
+                    }
+                    const int j_incl = __shfl_sync(kFull, incl, j);
+                    const int j_cnt = __shfl_sync(kFull, cnt, j);
+                    const int j_first = __shfl_sync(kFull, first, j);
+                    const int j_k = __shfl_sync(kFull, k, j);
+                    const int j_p = __shfl_sync(kFull, p, j);
+                    bool hit = false;
+                    if (t < L) {
+                        const int leaf = j_first + (t - (j_incl - j_cnt));
+                        float4 ls = table[table_index<M>(row0 + (size_t)j_k, G + leaf)];
+                        ls.w += kEnvInflate;
+                        hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
+                    }
+                    ++st.leaf;
+                    if constexpr (kOver) {
+                        const bool j_gate = __shfl_sync(kFull, (int)gate, j) != 0;
+                        if (__any_sync(kFull, hit && j_gate)) {
                             collide = true;
                             break;
                         }
-                        pend &= ~__ballot_sync(kFull, j_k == uk && j_g == ug);
-                    }
-                    if (collide) break;
-                } else {
-                    if (__any_sync(kFull, hit)) {
-                        collide = true;
-                        break;
+                        // Hits of overhanging leaves whose bound missed this primitive:
+                        // they count once the bound hits some primitive at that sample.
+                        const int j_g = __shfl_sync(kFull, g, j);
+                        uint32_t pend = __ballot_sync(kFull, hit);
+                        while (pend) {
+                            const int u = __ffs(pend) - 1;
+                            const int uk = __shfl_sync(kFull, j_k, u);
+                            const int ug = __shfl_sync(kFull, j_g, u);
+                            if (bound_hits_any<M>(table, row0, uk, ug, prim, np)) {
+                                collide = true;
+                                break;
+                            }
+                            pend &= ~__ballot_sync(kFull, j_k == uk && j_g == ug);
+                        }
+                        if (collide) break;
+                    } else {
+                        if (__any_sync(kFull, hit)) {
+                            collide = true;
+                            break;
+                        }
                     }
                 }
+                if (collide) break;
             }
-            if (collide) break;
+            c += dc;
+            r += dr;
+            if (c >= C) {
+                c -= C;
+                ++r;
+            }
         }
-        // Probe: once the chunk that completes rank 0 (the edge's first sample
-        // against every candidate, where most colliding pairs collide) is
-        // walked, queue the pair for the learned order only when much work
-        // remains; small remainders finish in plain order.
-        if (MODE == 1 && w0 == (((C - 1) >> 5) << 5) && total - (w0 + 32) >= queue_min_items && queue()) {
+        if (MODE != 1 || collide || w_stop >= total) break;
+        if (queue()) {
             undecided = true;
             break;
         }
-        c += dc;
-        r += dr;
-        if (c >= C) {
-            c -= C;
-            ++r;
-        }
+        w_stop = total;
     }
     if constexpr (MODE == 2) {
         if (collide && lane == 0) *stop = 1;

@@ -92,3 +92,31 @@ def test_negative_row_budget_is_rejected(checker, trained):
     checker.upload(workload.gen_envs("stress", 4, seed=42))
     with pytest.raises(Exception, match="learned_row_cap"):
         checker.check(workload.gen_edges("stress", 10, seed=42), order="learned", row_cap=-1)
+
+
+@pytest.mark.parametrize("warps,persistent", [(1, 0), (2, 1), (4, 0), (8, 1)])
+def test_finish_split_keeps_verdicts(checker, trained, warps, persistent):
+    """Threshold 0 queues every pair still undecided after its first sample;
+    the finish kernel splits each across 1, 2, 4 or 8 warps of its CTA.
+    Verdicts stay the plain order's and the work counters still count every
+    walked pair once."""
+    checker.mlp_set_params(trained["params"])
+    envs = workload.gen_envs("stress", 20, seed=51)
+    edges = workload.gen_edges("stress", 300, seed=51)
+    checker.upload(envs)
+    cfg = checker.launch_config()
+    try:
+        checker.set_launch_config(edges_per_cta=64, warps=warps, persistent=persistent, queue_min_items=0)
+        checker.set_profiling(True, counters=True)
+        plain = checker.check(edges, order="plain")
+        work_plain = checker.work_counters()
+        learned = checker.check(edges, order="learned")
+        work_learned = checker.work_counters()
+        checker.set_profiling(False)
+        assert np.array_equal(plain, learned)
+        assert checker.last_learned_pairs() > 0
+        assert work_learned["pairs"] == work_plain["pairs"]
+        assert work_learned["colliding"] == work_plain["colliding"]
+    finally:
+        checker.set_profiling(False)
+        checker.set_launch_config(**cfg)
