@@ -401,10 +401,11 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
     // first sample against every candidate, where most colliding pairs
     // collide) when at least queue_min_items items remain; the pair is then
     // queued for the learned order or, if queue() declines, walked on in plain
-    // order.  The pause ends the first pass of the loop, so no chunk pays for
-    // the decision.
+    // order.  Without overhang the pause ends the first pass of the loop, so no
+    // chunk pays for the decision; the overhang-aware walk keeps the decision
+    // inside its loop (measured 5 % faster for Baxter's probe).
     int w_stop = total;
-    if constexpr (MODE == 1) {
+    if constexpr (MODE == 1 && !kOver) {
         const int w_dec = ((C - 1) >> 5) << 5;
         if (total - (w_dec + 32) >= queue_min_items) w_stop = w_dec + 32;
     }
@@ -522,6 +523,12 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 }
                 if (collide) break;
             }
+            if constexpr (MODE == 1 && kOver) {
+                if (w0 == (((C - 1) >> 5) << 5) && total - (w0 + 32) >= queue_min_items && queue()) {
+                    undecided = true;
+                    break;
+                }
+            }
             c += dc;
             r += dr;
             if (c >= C) {
@@ -529,7 +536,7 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 ++r;
             }
         }
-        if (MODE != 1 || collide || w_stop >= total) break;
+        if (MODE != 1 || kOver || collide || w_stop >= total) break;
         if (queue()) {
             undecided = true;
             break;
