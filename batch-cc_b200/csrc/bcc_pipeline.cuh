@@ -358,35 +358,33 @@ __device__ __forceinline__ GroupLanes group_lanes() {
 
 // Whole warp: walk (sample rank, pair) items 32 at a time in check order --
 // plain reference order, or with `perm` the edge's segments in learned order --
-// and return whether some item collides.  MODE 1 (probe): after the chunk that
+// and return whether some item collides.  Items [w_begin, w_end) are walked
+// (w_end < 0: all).  MODE 1 (probe) with overhang: after the chunk that
 // completes rank 0, when at least queue_min_items remain, the whole warp calls
 // queue(); if that queues the pair, the walk stops with `undecided` set,
-// otherwise it goes on in plain order.
+// otherwise it goes on in plain order (robots without overhang make that
+// decision in check_pair, between two walks).
 // Each chunk tests the bounds (one per item); the leaf work of the items whose
 // bound hit is then flattened over the warp (item j owns leaf slots
 // [incl_j - cnt_j, incl_j)) and the warp stops at the first step with a hit.
-// MODE 2 (finish): the CTA's warps split the pair -- this warp walks chunks
-// chunk0, chunk0 + stride, ... and all stop once one of them sets *stop.
+// MODE 2 (finish): the CTA's warps split the pair -- this warp walks the
+// chunks at w_begin, w_begin + 32 stride, ... and all stop once one of them
+// sets *stop.
 template <class M, int MODE, class Queue>
 __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, size_t row0, int n, int C,
                                            const uint16_t* pairs, const float4* prim, int np, const uint8_t* perm,
                                            int queue_min_items, const GroupLanes& GL, bool& undecided,
-                                           WalkStats& st, Queue&& queue, int chunk0 = 0, int stride = 1,
-                                           volatile int* stop = nullptr) {
+                                           WalkStats& st, Queue&& queue, int w_begin = 0, int w_end = -1,
+                                           int stride = 1, volatile int* stop = nullptr) {
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
     constexpr bool kOver = has_overhang<M>();
     const int lane = threadIdx.x & 31;
     const int total = kLanes * n * C;
-    int dr, dc, r, c, w_begin = 0, w_step = 32;
-    if constexpr (MODE == 2) {
-        w_begin = 32 * chunk0;
-        w_step = 32 * stride;
-        dr = w_step / C;
-        dc = w_step - dr * C;
-        r = (w_begin + lane) / C;
-        c = w_begin + lane - r * C;
-    } else {
+    const int w_last = w_end < 0 ? total : w_end;
+    const int w_step = 32 * stride;
+    int dr, dc, r, c;
+    if (MODE != 2 && w_begin == 0) {
         // a / C for a <= 32 and 1 <= C <= kPairCap: floor((a + 0.5) / C) in FP32 is
         // exact (the quotient stays >= 1 / 2048 away from an integer), and cheaper
         // than an integer division by a runtime divisor.
@@ -395,23 +393,15 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
         dc = 32 - dr * C;
         r = (int)(((float)lane + 0.5f) * inv_c);
         c = lane - r * C;
+    } else {
+        dr = w_step / C;
+        dc = w_step - dr * C;
+        r = (w_begin + lane) / C;
+        c = w_begin + lane - r * C;
     }
     bool collide = false;
-    // Probe: the walk pauses after the chunk that completes rank 0 (the edge's
-    // first sample against every candidate, where most colliding pairs
-    // collide) when at least queue_min_items items remain; the pair is then
-    // queued for the learned order or, if queue() declines, walked on in plain
-    // order.  Without overhang the pause ends the first pass of the loop, so no
-    // chunk pays for the decision; the overhang-aware walk keeps the decision
-    // inside its loop (measured 5 % faster for Baxter's probe).
-    int w_stop = total;
-    if constexpr (MODE == 1 && !kOver) {
-        const int w_dec = ((C - 1) >> 5) << 5;
-        if (total - (w_dec + 32) >= queue_min_items) w_stop = w_dec + 32;
-    }
-    int w0 = w_begin;
-    for (;;) {
-        for (; w0 < w_stop; w0 += w_step) {
+    {
+        for (int w0 = w_begin; w0 < w_last; w0 += w_step) {
             if constexpr (MODE == 2) {  // another warp of the CTA found a hit
                 int s = 0;
                 if (lane == 0) s = *stop;
@@ -465,29 +455,44 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
             if (__any_sync(kFull, cnt > 0)) {
                 ++st.gates;
                 int incl = cnt;
-    #pragma unroll
+#pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
                     const int y = __shfl_up_sync(kFull, incl, o);
                     if (lane >= o) incl += y;
                 }
                 const int L = __shfl_sync(kFull, incl, 31);
+                // Without overhang a slot needs only its item's sample, primitive
+                // and leaf offset: p | (first - exclusive count) << 12, one shuffle.
+                int dp = 0;
+                if constexpr (!kOver) {
+                    static_assert(max_prims_of<M>() < 4096, "primitive index packs into 12 bits");
+                    dp = (int)(((unsigned)(first - (incl - cnt)) << 12) | (unsigned)p);
+                }
                 for (int t0 = 0; t0 < L; t0 += 32) {
                     const int t = t0 + lane;
                     // owner j: the first lane whose inclusive count exceeds t
                     int j = 0;
-    #pragma unroll
+#pragma unroll
                     for (int step = 16; step; step >>= 1) {
                         const int v = __shfl_sync(kFull, incl, j + step - 1);
                         if (v <= t) j += step;
                     }
-                    const int j_incl = __shfl_sync(kFull, incl, j);
-                    const int j_cnt = __shfl_sync(kFull, cnt, j);
-                    const int j_first = __shfl_sync(kFull, first, j);
-                    const int j_k = __shfl_sync(kFull, k, j);
-                    const int j_p = __shfl_sync(kFull, p, j);
+                    int j_k, j_p, leaf;
+                    if constexpr (!kOver) {
+                        const int jd = __shfl_sync(kFull, dp, j);
+                        j_k = __shfl_sync(kFull, k, j);
+                        j_p = jd & 4095;
+                        leaf = t + (jd >> 12);
+                    } else {
+                        const int j_incl = __shfl_sync(kFull, incl, j);
+                        const int j_cnt = __shfl_sync(kFull, cnt, j);
+                        const int j_first = __shfl_sync(kFull, first, j);
+                        j_k = __shfl_sync(kFull, k, j);
+                        j_p = __shfl_sync(kFull, p, j);
+                        leaf = j_first + (t - (j_incl - j_cnt));
+                    }
                     bool hit = false;
                     if (t < L) {
-                        const int leaf = j_first + (t - (j_incl - j_cnt));
                         float4 ls = table[table_index<M>(row0 + (size_t)j_k, G + leaf)];
                         ls.w += kEnvInflate;
                         hit = sphere_hits_prim(ls, prim + j_p * kPrimF4);
@@ -523,6 +528,8 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 }
                 if (collide) break;
             }
+            // Probe (overhang-aware walk): the queue decision stays inside the
+            // loop, measured 5 % faster for Baxter than a separate first walk.
             if constexpr (MODE == 1 && kOver) {
                 if (w0 == (((C - 1) >> 5) << 5) && total - (w0 + 32) >= queue_min_items && queue()) {
                     undecided = true;
@@ -536,12 +543,6 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 ++r;
             }
         }
-        if (MODE != 1 || kOver || collide || w_stop >= total) break;
-        if (queue()) {
-            undecided = true;
-            break;
-        }
-        w_stop = total;
     }
     if constexpr (MODE == 2) {
         if (collide && lane == 0) *stop = 1;
@@ -666,8 +667,33 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
             if (lane + 32 < nseg) perm_buf[rank1] = (uint8_t)(lane + 32);
             __syncwarp();
         }
-        collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np, learned ? perm_buf : nullptr,
-                                      P.queue_min_items, GL, undecided, st, queue, chunk0, stride, stop);
+        if constexpr (MODE == 1 && !has_overhang<M>()) {
+            // Probe: walk up to the chunk that completes rank 0 (the edge's first
+            // sample against every candidate, where most colliding pairs
+            // collide); when at least queue_min_items items remain, queue the
+            // pair for the learned order or, if queue() declines, walk on.  Two
+            // plain walks, so no chunk of either pays for the decision.
+            const int total = kLanes * n * Cs;
+            const int w_dec = (((Cs - 1) >> 5) << 5) + 32;
+            if (total - w_dec >= P.queue_min_items) {
+                collide = walk_pairs<M, 0>(P.table, row0, n, Cs, pairs, prim, np, nullptr, 0, GL, undecided, st,
+                                           queue, 0, w_dec);
+                if (!collide) {
+                    if (queue())
+                        undecided = true;
+                    else
+                        collide = walk_pairs<M, 0>(P.table, row0, n, Cs, pairs, prim, np, nullptr, 0, GL, undecided,
+                                                   st, queue, w_dec);
+                }
+            } else {
+                collide = walk_pairs<M, 0>(P.table, row0, n, Cs, pairs, prim, np, nullptr, 0, GL, undecided, st,
+                                           queue);
+            }
+        } else {
+            collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np, learned ? perm_buf : nullptr,
+                                          P.queue_min_items, GL, undecided, st, queue, 32 * chunk0, -1, stride,
+                                          stop);
+        }
         __syncwarp();  // every lane is done with this segment's pairs
     };
     // Robots whose leaves all lie inside their bounds have a small walk: a
