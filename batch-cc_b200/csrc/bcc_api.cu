@@ -824,8 +824,8 @@ bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg) {
 }
 
 // Time each candidate configuration on the given edges against the uploaded
-// environments (1 warm-up + the median of 5 timed graph replays, CUDA events,
-// L2 overwritten before each) and keep the fastest.
+// environments (1 capturing check + the median of 5 timed graph replays, CUDA
+// events, L2 overwritten before each) and keep the fastest.
 bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
                         int32_t order, int32_t* chosen) {
     if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
@@ -838,10 +838,12 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
     BCC_CUDA(ctx, ctx->edges.ensure(eb));
     BCC_CUDA(ctx, ctx->results.ensure((size_t)num_edges * ctx->num_envs));
     BCC_CUDA(ctx, cudaMemcpy(ctx->edges.p, edges, eb, cudaMemcpyHostToDevice));
-    // Graph replays, as a caller timing many checks runs them: one warm-up
-    // (capture), then the median of kTuneReps individually timed checks, each
-    // after L2 was overwritten (untimed) so that no check starts on the previous
-    // one's cached tables.
+    // One full check captures the configuration's graph (everything after the
+    // discretisation, which depends only on the edges); then the median of
+    // kTuneReps timed replays of that graph, each after L2 was overwritten
+    // (untimed) so that no replay starts on the previous one's cached tables.
+    // Timing the replays alone keeps the host's per-check work (the sample
+    // count read back) out of the comparison.
     constexpr int kTuneReps = 5;
     constexpr size_t kFlushBytes = 256u << 20;  // twice the L2
     bcc::DevBuf flush;
@@ -859,13 +861,19 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
         bcc_status s = run_check(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, ctx->results.as<uint8_t>(),
                                  &opts, st);
         if (s != BCC_OK) return s;
+        const bcc::GraphCache& G = ctx->graph[order == BCC_ORDER_LEARNED ? 1 : 0];
+        const bool replay = G.exec && !ctx->counting && same_tune(G.tune, t);  // the graph just captured
         float reps[kTuneReps];
         for (int r = 0; r < kTuneReps; ++r) {
             BCC_CUDA(ctx, cudaMemsetAsync(flush.p, r, kFlushBytes, st));
             BCC_CUDA(ctx, cudaEventRecord(e0, st));
-            s = run_check(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, ctx->results.as<uint8_t>(), &opts,
-                          st);
-            if (s != BCC_OK) return s;
+            if (replay) {
+                BCC_CUDA(ctx, cudaGraphLaunch(G.exec, st));
+            } else {  // no graph (work counters on): time the whole check
+                s = run_check(ctx, robot, ctx->edges.as<float>(), num_edges, resolution, ctx->results.as<uint8_t>(),
+                              &opts, st);
+                if (s != BCC_OK) return s;
+            }
             BCC_CUDA(ctx, cudaEventRecord(e1, st));
             BCC_CUDA(ctx, cudaEventSynchronize(e1));
             BCC_CUDA(ctx, cudaEventElapsedTime(&reps[r], e0, e1));
@@ -885,11 +893,16 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
             best = t;
         }
     };
-    // launch shape: edges per CTA x warps per CTA x persistent or not
-    auto sweep_launch = [&]() {
-        const int tiles[4] = {32, 64, 128, 256};
-        const int warps[2] = {4, 8};
-        const bcc::Tune base = best;
+    // Launch shape (edges per CTA x warps per CTA x persistent or not), and for
+    // the learned order jointly with the queue threshold: the shape that suits
+    // many queued pairs need not suit few, and a sweep of one at a time got
+    // stuck on a worse pair (Fetch: 3 % off).
+    const bool learned = order == BCC_ORDER_LEARNED && ctx->mlp.ready;
+    const int tiles[4] = {32, 64, 128, 256};
+    const int warps[2] = {4, 8};
+    const int qmins[6] = {128, 256, 512, 1024, 2048, 4096};
+    const bcc::Tune base = best;
+    for (int qi = 0; qi < (learned ? 6 : 1) && s == BCC_OK; ++qi)
         for (int ti = 0; ti < 4 && s == BCC_OK; ++ti)
             for (int wi = 0; wi < 2 && s == BCC_OK; ++wi)
                 for (int pe = 0; pe < 2 && s == BCC_OK; ++pe) {
@@ -897,22 +910,9 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
                     t.edges_per_cta = tiles[ti];
                     t.warps = warps[wi];
                     t.persistent = pe;
+                    if (learned) t.queue_min_items = qmins[qi];
                     keep(t);
                 }
-    };
-    sweep_launch();
-    if (s == BCC_OK && order == BCC_ORDER_LEARNED && ctx->mlp.ready) {
-        const int qmins[6] = {128, 256, 512, 1024, 2048, 4096};
-        const bcc::Tune base = best;
-        for (int qi = 0; qi < 6 && s == BCC_OK; ++qi) {
-            bcc::Tune t = base;
-            t.queue_min_items = qmins[qi];
-            keep(t);
-        }
-        // The shape that suits many queued pairs need not suit few: sweep it again
-        // at the chosen threshold.
-        if (s == BCC_OK) sweep_launch();
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ctx->profiling = saved_prof;

@@ -387,7 +387,9 @@ def run_ours(args, world, rank, local, dist):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
     # Autotuned launch configuration per order (untimed), on the first edges.
-    tuned = {o: chk.autotune(edges[:min(E, 10000)], order=o, robot=robot) for o in ("plain", "learned")}
+    # tuning subset: all edges up to 10 000, at most ~2e7 pairs per timed check
+    n_tune = min(E, 10000, max(1000, 20_000_000 // max(N, 1)))
+    tuned = {o: chk.autotune(edges[:n_tune], order=o, robot=robot) for o in ("plain", "learned")}
     if dist:
         dist.barrier()
     torch.cuda.synchronize()

@@ -237,9 +237,9 @@ bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg);
 bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg);
 /*
  * Autotuner: times candidate configurations (edges per CTA 32..256, 4 or 8
- * warps, persistent or not; for the learned order then the queue threshold
- * 128..4096 items and the launch shape once more at that threshold) on the
- * given host edges against the uploaded environments and keeps the fastest
+ * warps, persistent or not; for the learned order jointly with the queue
+ * threshold 128..4096 items) on the given host edges against the uploaded
+ * environments, timing graph replays, and keeps the fastest
  * in the context; chosen[4] receives it (may be NULL).  order: bcc_order.
  */
 bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
