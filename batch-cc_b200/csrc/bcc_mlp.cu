@@ -44,7 +44,8 @@ constexpr uint32_t kImgW = kMlpHidden * kMlpHidden * 2;    // 32768
 constexpr uint32_t kSmW1 = 0;
 constexpr uint32_t kSmW2 = kSmW1 + kImgW1;
 constexpr uint32_t kSmW3 = kSmW2 + kImgW;
-constexpr int kFwdGroups = 2;                              // independent 128-row tile streams per CTA
+constexpr int kFwdGroups = 3;                              // independent 128-row tile streams per CTA
+constexpr uint32_t kFwdTmemCols = 512;                     // power of two >= 128 x groups
 constexpr uint32_t kSmGroup0 = kSmW3 + kImgW;              // group g: X at +g*stride, H at +kImgW1
 constexpr uint32_t kSmGroupStride = kImgW1 + kImgW;
 constexpr uint32_t kSmVec = kSmGroup0 + kFwdGroups * kSmGroupStride;  // b1 b2 b3 w4 (4 x 128) + b4
@@ -53,6 +54,7 @@ constexpr uint32_t kSmTmem = kSmBar + 8 * kFwdGroups;
 constexpr uint32_t kFwdSmem = kSmTmem + 8;
 constexpr uint32_t kImagesBytes = kImgW1 + 2 * kImgW;       // W1T | W2T | W3T
 static_assert(kSmGroup0 % 16 == 0 && kSmGroupStride % 16 == 0, "core-matrix images are 16-byte aligned");
+static_assert(kFwdSmem <= 227 * 1024, "forward kernel shared memory");
 
 // ---------------------------------------------------------------- images
 // FP32 masters -> BF16 core-matrix images of W1^T [128][48], W2^T, W3^T.
@@ -122,10 +124,11 @@ __device__ __forceinline__ bool group_sync_or(bool pred, int grp) {
     return r != 0;
 }
 
-// Persistent: each CTA loads the weights once; its two warp groups (4 warps,
+// Persistent: each CTA loads the weights once; its three warp groups (4 warps,
 // one row per thread each) run independent streams of 128-row tiles, each with
 // its own X/H images, TMEM accumulator (columns 128 g ..) and mbarrier, so one
-// group's MMAs overlap the other's epilogue.  x: BF16 [rows][48] row-major;
+// group's MMAs overlap the others' epilogues (three groups measured 1.3x two:
+// the epilogues, not the MMAs, set the pace).  x: BF16 [rows][48] row-major;
 // logits: FP32 [rows].
 __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     mlp_forward_kernel(const uint16_t* __restrict__ x, int rows, const int* __restrict__ rows_dev,
@@ -156,7 +159,7 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
         for (int g = 0; g < kFwdGroups; ++g) mbar_init(reinterpret_cast<uint64_t*>(sm + kSmBar) + g, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) tc::tmem_alloc(tmem_slot, 128 * kFwdGroups);
+    if (warp == 0) tc::tmem_alloc(tmem_slot, kFwdTmemCols);
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
@@ -224,7 +227,7 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    if (warp == 0) tc::tmem_free(*tmem_slot, 128 * kFwdGroups);
+    if (warp == 0) tc::tmem_free(*tmem_slot, kFwdTmemCols);
 }
 
 // ---------------------------------------------------------------- training
