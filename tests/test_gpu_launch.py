@@ -61,4 +61,7 @@ def test_autotune_picks_a_valid_config(checker, case):
     assert cfg["edges_per_cta"] in (32, 64, 128, 256) and cfg["warps"] in (4, 8)
     assert np.array_equal(checker.check(edges), base)
     cfg = checker.autotune(edges, order="learned")
+    # the learned order's shape and queue threshold are swept jointly
+    assert cfg["edges_per_cta"] in (32, 64, 128, 256) and cfg["warps"] in (4, 8)
+    assert cfg["queue_min_items"] in (128, 256, 512, 1024, 2048, 4096)
     assert np.array_equal(checker.check(edges, order="learned"), base)
