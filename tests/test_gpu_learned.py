@@ -1,7 +1,7 @@
 """GPU tests of the learned check order: the trained proposal never changes a
 verdict, it is trained by the project's tensor-core kernels on checker labels,
 its misprediction rate is measured, and it reduces the work spent on the pairs
-a plain first chunk leaves undecided."""
+a plain probe of their first sample leaves undecided."""
 import numpy as np
 import pytest
 
