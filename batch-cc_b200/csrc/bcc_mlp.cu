@@ -171,15 +171,23 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     bool bad = false;
 
     const int tiles = (rows + 127) / 128;
-    for (int tile = blockIdx.x * kFwdGroups + grp; tile < tiles && !bad; tile += gridDim.x * kFwdGroups) {
+    const int tile_step = gridDim.x * kFwdGroups;
+    // X rows are loaded one tile ahead into registers, so their latency overlaps
+    // the current tile's three layers.
+    uint4 xv[kMlpIn / 8];
+    auto load_x = [&](int tile) {
         const int row = tile * 128 + gt;
-        // X tile: this thread's row, six 16-byte chunks of 8 features.
         const uint4* src = reinterpret_cast<const uint4*>(x + (size_t)row * kMlpIn);
 #pragma unroll
-        for (int j = 0; j < kMlpIn / 8; ++j) {
-            const uint4 v = row < rows ? src[j] : make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4*>(xs + tc::cm_offset(gt, 8 * j, kMlpIn)) = v;
-        }
+        for (int j = 0; j < kMlpIn / 8; ++j) xv[j] = (tile < tiles && row < rows) ? src[j] : make_uint4(0, 0, 0, 0);
+    };
+    load_x(blockIdx.x * kFwdGroups + grp);
+    for (int tile = blockIdx.x * kFwdGroups + grp; tile < tiles && !bad; tile += tile_step) {
+        const int row = tile * 128 + gt;
+        // X tile: this thread's row, six 16-byte chunks of 8 features.
+#pragma unroll
+        for (int j = 0; j < kMlpIn / 8; ++j) *reinterpret_cast<uint4*>(xs + tc::cm_offset(gt, 8 * j, kMlpIn)) = xv[j];
+        load_x(tile + tile_step);
         // Three layers: MMAs from the group's first thread, epilogue from all.
 #pragma unroll 1
         for (int layer = 0; layer < 3; ++layer) {
