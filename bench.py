@@ -432,12 +432,12 @@ def run_ours(args, world, rank, local, dist):
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
     h_res = torch.empty((E, N), dtype=torch.uint8).pin_memory().numpy()
     chk.set_launch_config(**tuned[head])
-    chk.check(h_edges, out=h_res, order=head, robot=robot)
+    chk.check(h_edges, out=h_res, order=head, robot=robot, graph=True)
     t_e2e = []
     for _ in range(max(3, min(args.steps, 5))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        chk.check(h_edges, out=h_res, order=head, robot=robot)
+        chk.check(h_edges, out=h_res, order=head, robot=robot, graph=True)
         t_e2e.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(dist, statistics.median(t_e2e), f"cuda:{dev}")
     mlp_ms, mlp_tf = mlp_roofline(chk, dev)
@@ -462,7 +462,8 @@ def run_ours(args, world, rank, local, dist):
             "gpu_launches": (6 + 9) * args.steps,  # plain: 6 launches per step; learned: 9
             "clocks": clk.summary()}
     line["e2e"] = {"value": world * N * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(edges.nbytes),
-                   "d2h_bytes_per_step": int(N * E)}
+                   "d2h_bytes_per_step": int(N * E),
+                   "path": "bcc_check (host edges in, host verdicts out; bcc_opts.use_graph = 1)"}
     # Roofline of the dominant kernel (environment check, plain order):
     # algorithmic FLOPs of the reference plain order per launch / mean
     # CUDA-event duration of the launch.
