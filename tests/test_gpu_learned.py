@@ -120,3 +120,24 @@ def test_finish_split_keeps_verdicts(checker, trained, warps, persistent):
     finally:
         checker.set_profiling(False)
         checker.set_launch_config(**cfg)
+
+
+@pytest.mark.parametrize("name", ["multi_fetch", "multi_baxter"])
+def test_learned_order_overhang_robots(checker, name):
+    """Fetch and Baxter take the overhang-aware walk in the probe (queue
+    decision inside the loop) and in the split finish; with threshold 0 many
+    pairs are queued, and every verdict must stay the plain order's."""
+    robot = workload.robot_of(name)
+    checker.mlp_set_params(mlp.init_params(61))
+    envs = workload.gen_envs(name, 64, seed=61)
+    edges = workload.gen_edges(name, 1000, seed=61)  # ~2 % of the pairs are collision-free
+    checker.upload(envs)
+    cfg = checker.launch_config()
+    try:
+        checker.set_launch_config(edges_per_cta=32, warps=4, persistent=0, queue_min_items=0)
+        plain = checker.check(edges, order="plain", robot=robot)
+        learned = checker.check(edges, order="learned", robot=robot)
+        assert checker.last_learned_pairs() > 0
+        assert np.array_equal(plain, learned)
+    finally:
+        checker.set_launch_config(**cfg)
