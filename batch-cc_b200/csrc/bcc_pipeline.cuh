@@ -173,6 +173,51 @@ __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges
     row_edge[row] = e;
 }
 
+// Row-major tables (tile 1): a thread's row is 16 * num_spheres contiguous
+// bytes, so per-thread stores would touch 32 rows per warp instruction.  One
+// warp per CTA computes its 32 rows into shared memory (odd float4 row stride,
+// conflict-free) and then copies the 32 consecutive rows out as one contiguous
+// block, 512 bytes per warp store.
+template <class M>
+__global__ void __launch_bounds__(32) fk_staged_kernel(const float* __restrict__ edges, int E,
+                                                       const int* __restrict__ steps,
+                                                       const int* __restrict__ offs,
+                                                       float4* __restrict__ table,
+                                                       int* __restrict__ row_edge) {
+    static_assert(M::table_tile == 1, "row-major tables only");
+    constexpr int NS = M::num_spheres;
+    constexpr int STRIDE = NS | 1;
+    extern __shared__ float4 srow[];  // [32][STRIDE]
+    const int total = offs[E];
+    const int base = blockIdx.x * 32;
+    const int row = base + (int)threadIdx.x;
+    if (row < total) {
+        int lo = 0, hi = E - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (offs[mid] <= row) lo = mid; else hi = mid - 1;
+        }
+        const int e = lo;
+        const int k = row - offs[e];
+        float s[M::dof], t[M::dof], q[M::dof];
+#pragma unroll
+        for (int j = 0; j < M::dof; ++j) {
+            s[j] = edges[(size_t)e * 2 * M::dof + j];
+            t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
+        }
+        edge_sample<M::dof>(s, t, steps[e], k, q);
+        fk_spheres<M>(q, srow + threadIdx.x * STRIDE);
+        row_edge[row] = e;
+    }
+    __syncwarp();
+    const int n = min(32, total - base) * NS;
+    float4* __restrict__ dst = table + (size_t)base * NS;
+    for (int i = threadIdx.x; i < n; i += 32) {
+        const int r = i / NS;
+        dst[i] = srow[r * STRIDE + (i - r * NS)];
+    }
+}
+
 // ------------------------------------------------------------------ 4. self
 __device__ __forceinline__ bool self_hit(float4 a, float4 b) {
     const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
@@ -1225,7 +1270,17 @@ cudaError_t run_prep(const PipelineArgs& a, cudaStream_t st) {
     const int R = a.total_rows;
     cudaEvent_t* ev = a.stage_events;
     if (ev) cudaEventRecord(ev[1], st);
-    if (R > 0) fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
+    if (R > 0) {
+        if constexpr (M::table_tile == 1) {
+            const size_t smem = 32 * (size_t)(M::num_spheres | 1) * sizeof(float4);
+            cudaError_t err = cudaFuncSetAttribute(fk_staged_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+            if (err != cudaSuccess) return err;
+            fk_staged_kernel<M><<<(R + 31) / 32, 32, smem, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
+        } else {
+            fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
+        }
+    }
     if (ev) cudaEventRecord(ev[2], st);
     cudaError_t err = cudaMemsetAsync(a.edge_self, 0, sizeof(int) * E, st);
     if (err != cudaSuccess) return err;
