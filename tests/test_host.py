@@ -127,3 +127,15 @@ def test_robot_ids_of_the_binding():
     assert [_rid(r) for r in ("panda", "fetch", "baxter")] == [0, 1, 2]
     assert _rid(7) == 7  # ids pass through (an unknown one is the library's to reject)
     assert ROBOTS == {"panda": 0, "fetch": 1, "baxter": 2}
+
+
+def test_opts_binding_matches_the_header():
+    """The ctypes mirror of bcc_opts has the header's fields, in order, all int32."""
+    text = open(os.path.join(ROOT, "include", "bcc.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = re.search(r"typedef struct bcc_opts \{(.*?)\} bcc_opts;", text, flags=re.S).group(1)
+    fields = re.findall(r"int32_t\s+(\w+);", body)
+    assert [f for f, _ in bcclib.BccOpts._fields_] == fields
+    assert all(t is ctypes.c_int32 for _, t in bcclib.BccOpts._fields_)
+    o = bcclib.make_opts("learned", use_graph=True, tile=0, row_cap=77)
+    assert (o.order, o.use_graph, o.tile_override, o.learned_row_cap) == (bcclib.ORDERS["learned"], 1, 0, 77)
