@@ -767,7 +767,19 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
     bool single = false;
     if constexpr (!has_overhang<M>()) single = C > 0 && C <= K;
     if (single) {
-        write_seg(0, C);
+        // the whole list fits: no segment bounds to test while writing
+        if (cnt > 0) {
+            int idx = off;
+            for (int w = 0; w < W; ++w) {
+                uint64_t m = mask_word(w);
+                while (m) {
+                    const int b = __ffsll((long long)m) - 1;
+                    pairs[idx++] = (uint16_t)(((w * 64 + b) << GB) | lane);
+                    m &= m - 1;
+                }
+            }
+        }
+        __syncwarp();
         walk_seg(C);
     } else {
         for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
