@@ -766,8 +766,9 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
     // bookkeeping out of it.  The overhang-aware walk stays in one copy.
     bool single = false;
     if constexpr (!has_overhang<M>()) single = C > 0 && C <= K;
-    if (single) {
-        // the whole list fits: no segment bounds to test while writing
+    // The whole list fits the buffer (the usual case): no segment bounds to test
+    // while writing.
+    auto write_all = [&]() {
         if (cnt > 0) {
             int idx = off;
             for (int w = 0; w < W; ++w) {
@@ -780,11 +781,17 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
             }
         }
         __syncwarp();
+    };
+    if (single) {
+        write_all();
         walk_seg(C);
     } else {
         for (int seg0 = 0; seg0 < C && !collide && !undecided; seg0 += K) {
             const int seg1 = min(C, seg0 + K);
-            write_seg(seg0, seg1);
+            if (C <= K)
+                write_all();
+            else
+                write_seg(seg0, seg1);
             walk_seg(seg1 - seg0);
         }
     }
