@@ -77,6 +77,7 @@ def lib():
                                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         L.bcc_mlp_evaluate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
+        L.bcc_env_code.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
         L.bcc_last_learned_rows.argtypes = [vp]
         L.bcc_last_learned_rows.restype = ctypes.c_int64
         L.bcc_last_learned_pairs.argtypes = [vp]
@@ -221,6 +222,12 @@ class Checker:
                                            len(edges), resolution, int(num_samples), ctypes.c_uint64(seed),
                                            m.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return dict(zip(("loss", "mispredict", "false_pos", "false_neg", "positive"), [float(v) for v in m]))
+
+    def env_code(self):
+        """The 32-value code of every uploaded environment, float32 [num_envs, 32]."""
+        out = np.zeros((self.num_envs, 32), np.float32)
+        self._raise(lib().bcc_env_code(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.num_envs))
+        return out
 
     def last_learned_rows(self):
         return int(lib().bcc_last_learned_rows(self._h))

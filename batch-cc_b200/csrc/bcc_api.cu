@@ -177,7 +177,8 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     BCC_CUDA(ctx, cudaMemcpyAsync(ctx->h_total, a.offs + E, sizeof(int), cudaMemcpyDeviceToHost, st));
     BCC_CUDA(ctx, cudaStreamSynchronize(st));
     const int total = *ctx->h_total;
-    // offs[] is int32: the scan wraps past 2^31; cap the sample table at 2^27 rows.
+    // offs[] is int32 and the scan saturates at INT32_MAX instead of wrapping, so
+    // an oversized total shows up here; cap the sample table at 2^27 rows.
     if (total < 0 || total > (1 << 27))
         return fail(ctx, BCC_ERR_LIMIT, "too many samples in one call (edges too long or non-finite)");
     const int NS = ops->num_spheres;
@@ -783,6 +784,21 @@ bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, i
     h_metrics[2] = (float)(fp / n);
     h_metrics[3] = (float)(fn / n);
     h_metrics[4] = (float)(pos / n);
+    return BCC_OK;
+}
+
+bcc_status bcc_env_code(bcc_ctx* ctx, float* h_code, int32_t num_envs) {
+    if (!ctx || !h_code) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs < 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (num_envs != ctx->num_envs) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "num_envs differs from the uploaded set");
+    if (num_envs == 0) return BCC_OK;
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    bcc_status s = ensure_env_code(ctx, st);
+    if (s != BCC_OK) return s;
+    BCC_CUDA(ctx, cudaMemcpyAsync(h_code, ctx->env_code.p, sizeof(float) * bcc::kEnvCode * (size_t)num_envs,
+                                  cudaMemcpyDeviceToHost, st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
     return BCC_OK;
 }
 

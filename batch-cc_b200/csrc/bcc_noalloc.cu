@@ -18,9 +18,14 @@
 // that overlap on the GPU (two streams, two threads) race on the arrays: issue
 // them one at a time.  The first call on each device does the per-device
 // set-up (resolving the arrays' device addresses and uploading the robot
-// tables); make that first call before any stream capture on that device.
+// tables).  No call can be made inside a stream capture: every call reads the
+// sample count back to the host and synchronises the stream.  The set-up is
+// done once per device for the life of the process, so a cudaDeviceReset after
+// the first call is not supported (the robot tables would be gone while the
+// set-up record says they are loaded).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/bcc.h"
@@ -99,6 +104,10 @@ extern "C" bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records,
         return BCC_ERR_LIMIT;
     if (num_edges == 0 || num_envs == 0) return BCC_OK;
     if (!d_records && max_prims_per_env > 0) return BCC_ERR_INVALID_ARGUMENT;
+    // The records are staged into shared memory by bulk copies, which need a
+    // 16-byte-aligned source: refuse a misaligned pointer before any launch.
+    if (max_prims_per_env > 0 && (reinterpret_cast<uintptr_t>(d_records) & 15u) != 0)
+        return BCC_ERR_INVALID_ARGUMENT;
     if (!d_env_offsets || !d_edges || !d_results) return BCC_ERR_INVALID_ARGUMENT;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BCC_ERR_CUDA;
@@ -106,8 +115,8 @@ extern "C" bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records,
     if (setup_device(dev, ops, s) != cudaSuccess) return BCC_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-    // Stale contents from the previous call: clear what must start at zero.
-    if (cudaMemsetAsync(s->edge_self, 0, sizeof(int) * num_edges, st) != cudaSuccess) return BCC_ERR_CUDA;
+    // Stale contents from the previous call: clear what must start at zero (the
+    // per-edge self-collision flags are cleared by the prep stage itself).
     if (cudaMemsetAsync(s->error, 0, sizeof(int), st) != cudaSuccess) return BCC_ERR_CUDA;
 
     bcc::PipelineArgs a{};

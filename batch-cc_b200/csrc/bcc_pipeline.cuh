@@ -877,9 +877,12 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
         }
         __syncthreads();
         if (threadIdx.x == 0) bulk_copy_g2s(smem, P.blobs + (size_t)__float_as_uint(h0.w), bytes, &bar);
-        if (!mbar_wait_bounded(&bar, 0u, 1u << 22)) {
+        // The whole CTA takes one path: if any thread gave up, all flag, wait once
+        // more (bounded) for the copy in flight, and return together.
+        const bool ok = mbar_wait_bounded(&bar, 0u, 1u << 22);
+        if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
-            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
+            mbar_wait_bounded(&bar, 0u, 1u << 22);
             return;
         }
     }
@@ -1145,9 +1148,11 @@ __global__ void __launch_bounds__(WARPS * 32) check_records_kernel(RecordsParams
         __syncthreads();
         if (threadIdx.x == 0)
             bulk_copy_g2s(smem, P.records + (size_t)p_begin * kPrimF4, (uint32_t)np * kPrimF4 * 16u, &bar);
-        if (!mbar_wait_bounded(&bar, 0u, 1u << 22)) {
+        // One path for the whole CTA (see check_kernel).
+        const bool ok = mbar_wait_bounded(&bar, 0u, 1u << 22);
+        if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(P.error_flag, 1);
-            mbar_wait_bounded(&bar, 0u, 1u << 22);  // do not exit under an in-flight copy
+            mbar_wait_bounded(&bar, 0u, 1u << 22);
             return;
         }
     }

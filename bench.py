@@ -62,6 +62,47 @@ def workload_name(name, N, E):
     return "%s: %s, %d envs (%s) x %d edges (%s)" % (name, w["robot"], N, prims, E, edges)
 
 
+def bench_config(name, N, E, world):
+    """The workload description both arms print, key for key."""
+    return {"workload": "%s, resolution 32" % workload_name(name, N, E), "envs": N, "edges_per_gpu": E,
+            "resolution": 32, "l2": "256 MB buffer written between timed steps (untimed)",
+            "parallelism": "dp%d" % world}
+
+
+def parity_vs_reference(envs, edges, verdicts, robot, iters=3):
+    """Checker leg, untimed and after the timed region: the reference's own CUDA
+    kernel batch_cc_kernel<Robot> (src/batch_cc.cu:74-133, built unmodified from
+    the reference sources into oracle/_ref) on the same inputs; every verdict of
+    each order is compared with it and each mismatch adjudicated by the FP64
+    signed penetration of the pair (oracle): within 1e-5 m of contact it is
+    tolerated, beyond it counts as out of tolerance.  Also returns the reference
+    kernel's throughput, CUDA-event timed (mean of `iters` launches).  (None,
+    None) when the reference harness was not built."""
+    from oracle import oracle as orc
+    from oracle import ref
+    if not ref.available():
+        return None, None
+    N, E = envs.num_envs, len(edges)
+    ms, want = ref.time_kernel(envs, edges, iters=iters, robot=robot)
+    par = {"pairs": int(want.size),
+           "vs": "reference CUDA batch_cc_kernel<%s> (src/batch_cc.cu:74-133), built from the reference sources"
+                 % robot.capitalize(),
+           "tolerance": "mismatch tolerated when the FP64 penetration of the pair is within 1e-5 m of contact"}
+    worst = 0
+    for order, got in verdicts.items():
+        n_mis, n_adj, bad = orc.adjudicate(envs, edges, got, want, robot=robot)
+        par[order] = {"mismatches": int(n_mis), "mismatches_adjudicated": int(n_adj),
+                      "mismatches_out_of_tolerance": int(len(bad))}
+        worst = max(worst, int(len(bad)))
+        par.setdefault("mismatches_adjudicated", 0)
+        par["mismatches_adjudicated"] = max(par["mismatches_adjudicated"], int(n_adj))
+    par["mismatches_out_of_tolerance"] = worst
+    ref_cuda = {"value": N * E / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+                "timing": "CUDA events around the reference kernel launch, mean of %d" % iters,
+                "kernel": "batch_cc_kernel<%s>, <<<N*E, 32>>>" % robot.capitalize()}
+    return par, ref_cuda
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -76,6 +117,8 @@ def parse():
     p.add_argument("--train-envs", type=int, default=4000)
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the full-size parity leg against the reference "
+                                                             "CUDA kernel")
     p.add_argument("--flop-sample", type=int, default=20000)
     p.add_argument("--profile-order", default=None, choices=["plain", "learned"],
                    help="profiling run: only `--warmup` + `--steps` eager checks in this order (launch config "
@@ -215,7 +258,7 @@ def run_reference(args, world, rank):
     envs = workload.gen_envs(args.workload, args.envs, seed=0)
     edges = workload.gen_edges(args.workload, args.edges, seed=0)
     N, E = envs.num_envs, len(edges)
-    cfg = {"workload": workload_name(args.workload, N, E), "envs": N, "edges": E, "resolution": 32}
+    cfg = bench_config(args.workload, N, E, world)
     if args.ref_path == "cuda":
         from oracle import ref
         if not ref.available():
@@ -413,6 +456,7 @@ def run_ours(args, world, rank, local, dist):
                      robot=robot)
     torch.cuda.synchronize()
     mismatch = int((d_res != d_res2).sum().item())
+    verdicts = {"plain": d_res.cpu().numpy(), "learned": d_res2.cpu().numpy()}
     work = {}
     chk.set_profiling(True, counters=True)
     for order in ("plain", "learned"):
@@ -449,9 +493,7 @@ def run_ours(args, world, rank, local, dist):
             "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
-            "config": {"workload": "%s, resolution 32, %s-ordered" % (workload_name(args.workload, N, E), head),
-                       "envs": N, "edges_per_gpu": E, "order": head,
-                       "l2": "256 MB buffer written between timed steps (untimed)", "parallelism": "dp%d" % world},
+            "config": bench_config(args.workload, N, E, world), "order": head,
             "orders": {o: {"value": world * N * E / (ms[o] * 1e-3), "ms_per_step": ms[o],
                            "launch": dict(tuned[o], graph=True), "stages_ms_per_step_eager": results[o][2],
                            "work_per_pair": work[o]} for o in results},
@@ -492,6 +534,11 @@ def run_ours(args, world, rank, local, dist):
                             "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst) of measured" if bf16_peak else
                             "fallback 1590 TFLOP/s (an earlier cuBLAS BF16 measurement on these B200s; "
                             "MEASURED_PEAKS.json absent)"}
+    if not args.no_parity:
+        par, ref_cuda = parity_vs_reference(envs, edges, verdicts, robot)
+        if par is not None:
+            line["parity"] = par
+            line["reference_cuda"] = ref_cuda
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(envs, edges, robot)
     chk.close()

@@ -167,10 +167,14 @@ int32_t bcc_work_counters(bcc_ctx* ctx, uint64_t* out, int32_t max_counters);
  *     uint8[num_edges][num_envs], same meaning and layout as bcc_check.
  * Limits: num_edges <= 1024 and at most 4096 discretised samples per call
  * (sum over edges of 32 n); beyond either the call returns BCC_ERR_LIMIT
- * without checking anything.  Synchronous on `stream`.  The first call on a
- * device sets that device up (resolves the arrays' addresses, uploads the robot
- * tables): make it before any stream capture.  Every call reuses the same
- * arrays, so calls that overlap on the GPU race; issue them one at a time.
+ * without checking anything.  d_records must be 16-byte aligned (bulk copies
+ * stage it); a misaligned pointer returns BCC_ERR_INVALID_ARGUMENT before any
+ * launch.  Synchronous on `stream`: every call reads the sample count back and
+ * synchronises, so no call can be made inside a stream capture.  The first call
+ * on a device sets that device up for the life of the process (resolves the
+ * arrays' addresses, uploads the robot tables); a cudaDeviceReset after it is
+ * not supported.  Every call reuses the same arrays, so calls that overlap on
+ * the GPU race; issue them one at a time.
  */
 bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records, const int32_t* d_env_offsets,
                              int32_t num_envs, int32_t max_prims_per_env, const float* d_edges,
@@ -212,6 +216,14 @@ bcc_status bcc_mlp_train(bcc_ctx* ctx, bcc_robot robot, const float* edges, int3
  * false-negative rate, [4] positive fraction. */
 bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
                             int64_t num_samples, uint64_t seed, float* h_metrics);
+/* The 32-value environment code of every uploaded environment (the MLP's
+ * environment features), h_code: host float[num_envs][32], num_envs as
+ * uploaded.  [0..2] counts of sphere-, capsule- and box-like primitives / 64,
+ * [3] total / 64; [4 + 3a + k] for anchor a = (+-0.35, +-0.35, 0.3 | 0.8) m
+ * (bit 0: x, bit 1: y, bit 2: z) the signed distance to the nearest primitive
+ * of kind k, clamped to [-0.5, 1.5] m (1.5 without one); [28..30] mean centre,
+ * [31] mean rounding radius + half-extent sum. */
+bcc_status bcc_env_code(bcc_ctx* ctx, float* h_code, int32_t num_envs);
 /* MLP rows (segments) scored by the last learned-order check. */
 int64_t bcc_last_learned_rows(const bcc_ctx* ctx);
 /* (environment, edge) pairs the last learned-order check queued for the MLP

@@ -556,4 +556,32 @@ int orc_pair_flops(const bcc_env_soa* envs, int robot, const float* edges, int r
     });
 }
 
+// Per-sample verdicts of listed (edge, env) pairs: out[k * max_samples + j] = 1
+// when sample j (index order j = lane * n + round) of pair k collides, 0 when
+// it is free, 2 past the pair's 32 n samples (or when 32 n > max_samples).
+int orc_pair_samples(const bcc_env_soa* envs, int robot, const float* edges, int resolution,
+                     const int64_t* pairs, int num_pairs, int max_samples, int precision, int nthreads,
+                     uint8_t* out) {
+    return with_robot(robot, -1, [&](auto m) {
+        using M = decltype(m);
+        auto views = make_views(envs);
+        parallel_for(num_pairs, nthreads, [&](int64_t k) {
+            int64_t e = pairs[2 * k], v = pairs[2 * k + 1];
+            const float* edge = edges + e * 2 * M::dof;
+            Disc d = discretise(edge, edge + M::dof, M::dof, resolution);
+            uint8_t* o = out + k * (int64_t)max_samples;
+            std::fill(o, o + max_samples, (uint8_t)2);
+            if ((int64_t)kLanes * d.n > max_samples) return;
+            float q[16];
+            for (int t = 0; t < kLanes; ++t)
+                for (int i = 0; i < d.n; ++i) {
+                    sample_q(d, M::dof, t, i, q);
+                    o[t * d.n + i] = precision == 32 ? (uint8_t)config_collides<M, float>(views[v], q)
+                                                     : (uint8_t)config_collides<M, double>(views[v], q);
+                }
+        });
+        return 0;
+    });
+}
+
 }  // extern "C"

@@ -42,6 +42,8 @@ def lib():
         L.orc_robot_num_spheres.argtypes = [ctypes.c_int]
         L.orc_pair_flops.argtypes = [vp, ctypes.c_int, f32p, ctypes.c_int, i64p, ctypes.c_int,
                                      ctypes.c_int, f64p, u8p]
+        L.orc_pair_samples.argtypes = [vp, ctypes.c_int, f32p, ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, u8p]
         _lib = L
     return _lib
 
@@ -150,3 +152,21 @@ def pair_flops(envset, edges, pairs, resolution=32, nthreads=None, robot="panda"
     lib().orc_pair_flops(ctypes.byref(soa), ROBOTS[robot], _ptr(edges, ctypes.c_float), resolution,
                          _ptr(pairs, ctypes.c_int64), K, nt, _ptr(fl, ctypes.c_double), _ptr(v, ctypes.c_uint8))
     return fl, v
+
+
+def pair_samples(envset, edges, pairs, resolution=32, max_samples=None, precision=64, nthreads=None, robot="panda"):
+    """Per-sample verdicts uint8 [K, max_samples] of (edge, env) pairs: 1 collides, 0 free,
+    2 past the pair's 32 n samples; sample index j = lane * n + round."""
+    edges = _f32(edges)
+    pairs = np.ascontiguousarray(pairs, np.int64).reshape(-1, 2)
+    K = len(pairs)
+    if max_samples is None:
+        max_samples = 32 * max([edge_n(edges[e, 0], edges[e, 1], resolution) for e in set(pairs[:, 0].tolist())] + [1])
+    out = np.full((K, max_samples), 2, np.uint8)
+    if K == 0:
+        return out
+    soa = envset.as_ctypes()
+    nt = nthreads or os.cpu_count() or 1
+    lib().orc_pair_samples(ctypes.byref(soa), ROBOTS[robot], _ptr(edges, ctypes.c_float), resolution,
+                           _ptr(pairs, ctypes.c_int64), K, max_samples, precision, nt, _ptr(out, ctypes.c_uint8))
+    return out

@@ -54,6 +54,19 @@ def test_halton_matches_recurrence(dropin_bin):
     assert np.allclose(got[:4, 0], [1 / 3, 2 / 3, 1 / 9, 4 / 9])
 
 
+def test_halton_matches_reference_header(tmp_path):
+    """The drop-in header against the reference's own src/random/halton.hh:
+    1,000,010 draws per dimension (7, 8, 14), past the restart after
+    max_iterations, identical bit for bit (fixture made by
+    tests/golden/make_halton.py from the reference header)."""
+    exe = str(tmp_path / "halton_draws")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "halton_draws.cpp"), "-o", exe])
+    got = subprocess.check_output([exe], text=True)
+    want = open(os.path.join(GOLDEN, "halton_reference.txt")).read()
+    assert got == want
+
+
 def test_scale_cfg(dropin_bin):
     out = subprocess.check_output([dropin_bin, "scale"], text=True)
     got = np.array([float(v) for v in out.split()], np.float32)

@@ -189,6 +189,24 @@ def test_checker_matches_reference_cuda_path(checker, name, nenv, nedge, seed):
     assert_parity(envs, edges, orc.check(envs, edges, robot=robot), want, "oracle vs reference CUDA", robot)
 
 
+@pytest.mark.skipif(not ref.available(), reason="reference harness not built")
+def test_full_size_parity_vs_reference_cuda(checker):
+    """Every (env, edge) pair of the full-size uneven workload (1000 envs x
+    10000 edges, seed 0): both check orders against the reference's own public
+    API batch_cc::batch_cc<Panda> (its CUDA kernel), each mismatch adjudicated
+    by the FP64 penetration; none may lie beyond 1e-5 m of contact."""
+    from bcc import mlp
+    envs = workload.gen_envs("uneven", seed=0)
+    edges = workload.gen_edges("uneven", seed=0)
+    want = ref.check(envs, edges)
+    checker.upload(envs)
+    checker.mlp_set_params(mlp.init_params(3))
+    for order in ("plain", "learned"):
+        got = checker.check(edges, order=order)
+        n_mis = assert_parity(envs, edges, got, want, "full size vs reference CUDA, %s order" % order)
+        assert n_mis < 1e-4 * want.size, (order, n_mis)
+
+
 def test_full_size_properties(checker):
     """Uneven workload at full size (1000 envs x 10000 edges): deterministic,
     and a random sample of pairs agrees with the oracle."""

@@ -98,4 +98,8 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
     d_edges = torch.from_numpy(long_edges).cuda()
     assert fn(0, d_rec.data_ptr(), d_off.data_ptr(), 2, max_prims, d_edges.data_ptr(), 200, 32,
               d_res.data_ptr(), stream) == 6
+    # Records 4 bytes off a 16-byte boundary: refused on the host before any launch.
+    d_edges = torch.from_numpy(workload.gen_edges("uneven", 8, seed=45)).cuda()
+    assert fn(0, d_rec.data_ptr() + 4, d_off.data_ptr(), 2, max_prims, d_edges.data_ptr(), 8, 32,
+              d_res.data_ptr(), stream) == 1  # BCC_ERR_INVALID_ARGUMENT
     torch.cuda.synchronize()
