@@ -78,6 +78,14 @@ def lib():
         L.bcc_mlp_evaluate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)]
         L.bcc_env_code.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
+        L.bcc_mlp_train_queued.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_float, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                           ctypes.POINTER(ctypes.c_int64)]
+        L.bcc_mlp_rank_metrics.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.c_int32]
         L.bcc_last_learned_rows.argtypes = [vp]
         L.bcc_last_learned_rows.restype = ctypes.c_int64
         L.bcc_last_learned_pairs.argtypes = [vp]
@@ -215,6 +223,35 @@ class Checker:
                                         ctypes.byref(pos)))
         return losses, float(pos.value)
 
+    def mlp_train_queued(self, edges, num_samples, queue_min_items=128, epochs=2, batch=16384, lr=2e-3, seed=0,
+                         resolution=32, robot="panda"):
+        """Train on the segments of the pairs the learned order's probe queues (threshold queue_min_items)
+        over the uploaded envs; returns (epoch losses, positive fraction, rows used)."""
+        edges = np.ascontiguousarray(edges, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        pos = ctypes.c_float(0)
+        rows = ctypes.c_int64(0)
+        self._raise(lib().bcc_mlp_train_queued(
+            self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(edges), resolution,
+            int(queue_min_items), int(num_samples), epochs, batch, ctypes.c_float(lr), ctypes.c_uint64(seed),
+            losses.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(pos), ctypes.byref(rows)))
+        return losses, float(pos.value), int(rows.value)
+
+    RANK_METRICS = ("queued_pairs", "scored_segments", "colliding_pairs", "colliding_samples", "auc",
+                    "ranks_to_hit_plain", "ranks_to_hit_learned", "ranks_to_hit_perfect",
+                    "ranks_walked_plain", "ranks_walked_learned", "ranks_walked_perfect", "realised_share",
+                    "mispredict")
+
+    def mlp_rank_metrics(self, edges, queue_min_items=128, resolution=32, robot="panda"):
+        """Ranking quality of the current network on the learned order's population (bcc_mlp_rank_metrics)."""
+        edges = np.ascontiguousarray(edges, np.float32)
+        m = np.zeros(13, np.float64)
+        self._raise(lib().bcc_mlp_rank_metrics(self._h, _rid(robot),
+                                               edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(edges),
+                                               resolution, int(queue_min_items),
+                                               m.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 13))
+        return dict(zip(self.RANK_METRICS, [float(v) for v in m]))
+
     def mlp_evaluate(self, edges, num_samples, seed=1, resolution=32, robot="panda"):
         edges = np.ascontiguousarray(edges, np.float32)
         m = np.zeros(5, np.float32)
@@ -235,22 +272,23 @@ class Checker:
     def last_learned_pairs(self):
         return int(lib().bcc_last_learned_pairs(self._h))
 
-    CONFIG = ("edges_per_cta", "warps", "persistent", "queue_min_items")
+    CONFIG = ("edges_per_cta", "warps", "persistent", "queue_min_items", "finish_split", "learned_mode",
+              "clusters")
 
     def launch_config(self):
-        c = (ctypes.c_int32 * 4)()
+        c = (ctypes.c_int32 * len(self.CONFIG))()
         self._raise(lib().bcc_get_launch_config(self._h, c))
         return dict(zip(self.CONFIG, list(c)))
 
     def set_launch_config(self, **kw):
         cfg = self.launch_config()
         cfg.update(kw)
-        c = (ctypes.c_int32 * 4)(*[int(cfg[k]) for k in self.CONFIG])
+        c = (ctypes.c_int32 * len(self.CONFIG))(*[int(cfg[k]) for k in self.CONFIG])
         self._raise(lib().bcc_set_launch_config(self._h, c))
 
     def autotune(self, edges, order="plain", resolution=32, robot="panda"):
         edges = np.ascontiguousarray(edges, np.float32)
-        c = (ctypes.c_int32 * 4)()
+        c = (ctypes.c_int32 * len(self.CONFIG))()
         self._raise(lib().bcc_autotune(self._h, _rid(robot), edges.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                        len(edges), resolution, ORDERS[order], c))
         return dict(zip(self.CONFIG, list(c)))

@@ -11,7 +11,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -206,6 +208,7 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
         a.edges_per_cta = (E + 65534) / 65535;
     a.persistent = ctx->tune.persistent;
     a.queue_min_items = ctx->tune.queue_min_items;
+    a.finish_split = ctx->tune.finish_split;
     BCC_CUDA(ctx, ctx->work_counter.ensure(64));
     a.work_counter = ctx->work_counter.as<int>();
     return BCC_OK;
@@ -218,6 +221,70 @@ bcc_status ensure_env_code(bcc_ctx* ctx, cudaStream_t st) {
     BCC_CUDA(ctx, bcc::launch_env_encode(ctx->blobs.as<float4>(), ctx->env_hdr.as<float4>(), ctx->num_envs,
                                          ctx->env_code.as<float>(), st));
     ctx->env_code_ready = true;
+    return BCC_OK;
+}
+
+// Environment clusters of the inline learned order: k-means (Lloyd, 20
+// iterations) over the uploaded set's 32-value codes, K = min(tune.clusters,
+// num_envs), seeded deterministically by farthest-point selection from
+// environment 0.  The MLP scores each edge's segments once per cluster, with
+// the centroid as the environment code.  Recomputed when K changes or the set
+// is replaced.  Synchronous (host k-means); called outside any stream capture.
+bcc_status ensure_env_clusters(bcc_ctx* ctx, cudaStream_t st) {
+    const int N = ctx->num_envs;
+    const int K = std::max(1, std::min(ctx->tune.clusters, N));
+    if (ctx->cluster_k == K) return BCC_OK;
+    bcc_status s = ensure_env_code(ctx, st);
+    if (s != BCC_OK) return s;
+    constexpr int D = bcc::kEnvCode;
+    std::vector<float> code((size_t)N * D);
+    BCC_CUDA(ctx, cudaMemcpyAsync(code.data(), ctx->env_code.p, sizeof(float) * code.size(), cudaMemcpyDeviceToHost,
+                                  st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    auto d2 = [&](const float* a, const float* b) {
+        double t = 0;
+        for (int j = 0; j < D; ++j) t += (double)(a[j] - b[j]) * (a[j] - b[j]);
+        return t;
+    };
+    std::vector<float> cen((size_t)K * D);
+    std::vector<double> best((size_t)N, 1e300);
+    int pick = 0;
+    for (int k = 0; k < K; ++k) {
+        std::copy(&code[(size_t)pick * D], &code[(size_t)pick * D] + D, &cen[(size_t)k * D]);
+        int far = 0;
+        for (int i = 0; i < N; ++i) {
+            best[i] = std::min(best[i], d2(&code[(size_t)i * D], &cen[(size_t)k * D]));
+            if (best[i] > best[far]) far = i;
+        }
+        pick = far;
+    }
+    std::vector<int> id((size_t)N, 0);
+    for (int it = 0; it < 20; ++it) {
+        for (int i = 0; i < N; ++i) {
+            double bd = 1e300;
+            for (int k = 0; k < K; ++k) {
+                const double v = d2(&code[(size_t)i * D], &cen[(size_t)k * D]);
+                if (v < bd) {
+                    bd = v;
+                    id[i] = k;
+                }
+            }
+        }
+        std::vector<double> sum((size_t)K * D, 0.0);
+        std::vector<int> cnt((size_t)K, 0);
+        for (int i = 0; i < N; ++i) {
+            cnt[id[i]] += 1;
+            for (int j = 0; j < D; ++j) sum[(size_t)id[i] * D + j] += code[(size_t)i * D + j];
+        }
+        for (int k = 0; k < K; ++k)
+            if (cnt[k] > 0)  // an empty cluster keeps its centroid
+                for (int j = 0; j < D; ++j) cen[(size_t)k * D + j] = (float)(sum[(size_t)k * D + j] / cnt[k]);
+    }
+    BCC_CUDA(ctx, ctx->env_cluster.ensure(sizeof(int) * (size_t)std::max(N, 1)));
+    BCC_CUDA(ctx, ctx->centroids.ensure(sizeof(float) * cen.size()));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->env_cluster.p, id.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->centroids.p, cen.data(), sizeof(float) * cen.size(), cudaMemcpyHostToDevice));
+    ctx->cluster_k = K;
     return BCC_OK;
 }
 
@@ -249,6 +316,7 @@ bcc_status prepare_learned(bcc_ctx* ctx, bcc::PipelineArgs& a, int row_cap) {
     a.queue_min_items = ctx->tune.queue_min_items;
     a.finish_counter = a.work_counter + 1;
     ctx->learned_rows_dev = reinterpret_cast<int*>(a.q_head);  // the low word counts rows
+    ctx->last_learned_inline = false;
     ctx->learned_row_cap = cap;
     ctx->learned_q_cap = q_cap;
     return BCC_OK;
@@ -275,17 +343,61 @@ bcc_status run_learned(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::PipelineArgs
     return BCC_OK;
 }
 
+// Inline learned order: buffers for K x segments MLP rows and the
+// per-(cluster, edge) 32-block permutations, sized outside any stream capture.
+bcc_status prepare_inline(bcc_ctx* ctx, bcc::PipelineArgs& a) {
+    bcc_status s = ensure_env_clusters(ctx, ctx->stream);
+    if (s != BCC_OK) return s;
+    const int K = ctx->cluster_k;
+    a.total_segs = a.total_rows / bcc::kSegment;
+    const size_t rows = (size_t)K * std::max(a.total_segs, 1);
+    if (rows > (size_t)kLearnedRowCap * 4)
+        return fail(ctx, BCC_ERR_LIMIT, "too many (cluster, segment) rows for the inline learned order");
+    BCC_CUDA(ctx, ctx->mlp.x.ensure(sizeof(uint16_t) * bcc::kMlpIn * rows));
+    BCC_CUDA(ctx, ctx->mlp.logits.ensure(sizeof(float) * rows));
+    BCC_CUDA(ctx, ctx->perms.ensure((size_t)K * std::max(a.num_edges, 1) * bcc::kLanes));
+    a.logits = ctx->mlp.logits.as<float>();
+    a.env_cluster = ctx->env_cluster.as<int>();
+    a.perms = ctx->perms.as<uint8_t>();
+    a.row_cap = (int)rows;
+    ctx->last_inline_rows = (long long)rows;
+    ctx->last_learned_inline = true;
+    return BCC_OK;
+}
+
+// Inline learned order: FK / self / swept, features of every (cluster,
+// segment) row, tcgen05 MLP scores, per-(cluster, edge) permutations, then one
+// check in which every pair walks rank 0 (sample 0) and then its other samples
+// in its cluster's learned order (mode 4): no queue, no second pass.
+bcc_status run_learned_inline(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::PipelineArgs& a, cudaStream_t st) {
+    cudaEvent_t* ev = a.stage_events;
+    BCC_CUDA(ctx, ops->prep(a, st));  // records stage events 1-4
+    const int K = ctx->cluster_k;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    BCC_CUDA(ctx, ops->cluster_features(a, ctx->centroids.as<float>(), K, ctx->mlp.x.as<uint16_t>(), st));
+    BCC_CUDA(ctx, bcc::mlp_forward(ctx->mlp.x.as<uint16_t>(), a.row_cap, ctx->mlp.images.as<uint8_t>(),
+                                   ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
+                                   std::max(sms, 1), st));
+    BCC_CUDA(ctx, ops->cluster_perms(a, K, ctx->perms.as<uint8_t>(), st));
+    a.mode = 4;
+    BCC_CUDA(ctx, ops->check_mode(a, st));
+    if (ev) cudaEventRecord(ev[5], st);
+    return BCC_OK;
+}
+
 bcc_status launch_sequence(bcc_ctx* ctx, bcc_robot robot, bcc::PipelineArgs& a, bool learned, cudaStream_t st) {
     const bcc::RobotOps* ops = bcc::robot_ops((int)robot);
     if (!ops) return fail(ctx, BCC_ERR_NOT_SUPPORTED, "robot not built into this library");
-    if (learned) return run_learned(ctx, ops, a, st);
+    if (learned) return ctx->tune.learned_mode == 0 ? run_learned_inline(ctx, ops, a, st) : run_learned(ctx, ops, a, st);
     BCC_CUDA(ctx, ops->check(a, st));
     return BCC_OK;
 }
 
 bool same_tune(const bcc::Tune& x, const bcc::Tune& y) {
     return x.edges_per_cta == y.edges_per_cta && x.warps == y.warps && x.persistent == y.persistent &&
-           x.queue_min_items == y.queue_min_items;
+           x.queue_min_items == y.queue_min_items && x.finish_split == y.finish_split &&
+           x.learned_mode == y.learned_mode && x.clusters == y.clusters;
 }
 
 bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution,
@@ -301,7 +413,7 @@ bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E,
         if (s != BCC_OK) return s;
         if (opts->learned_row_cap < 0)
             return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned_row_cap must be >= 0");
-        s = prepare_learned(ctx, a, opts->learned_row_cap);
+        s = ctx->tune.learned_mode == 0 ? prepare_inline(ctx, a) : prepare_learned(ctx, a, opts->learned_row_cap);
         if (s != BCC_OK) return s;
     }
     const bool graph = opts && opts->use_graph && !ctx->counting && !(opts->tile_override > 0);
@@ -638,6 +750,7 @@ bcc_status bcc_upload_envs(bcc_ctx* ctx, const bcc_env_soa* envs) {
     BCC_CUDA(ctx, ctx->grid_bounds.ensure(sizeof(A.bnd)));
     BCC_CUDA(ctx, cudaMemcpy(ctx->grid_bounds.p, A.bnd, sizeof(A.bnd), cudaMemcpyHostToDevice));
     ctx->env_code_ready = false;
+    ctx->cluster_k = 0;
     ctx->env_version += 1;
     return BCC_OK;
 }
@@ -787,6 +900,220 @@ bcc_status bcc_mlp_evaluate(bcc_ctx* ctx, bcc_robot robot, const float* edges, i
     return BCC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The learned order's population over the uploaded environments and the given
+// host edges: the probe (plain walk of every pair's rank 0, queue threshold
+// min_items) queues the pairs still undecided with at least min_items items
+// left; each segment of a queued pair gets its MLP feature row (mlp.x, at its
+// scored sample), each sample its environment verdict (mlp.lab, 8 per row) and
+// each scored sample its label (mlp.y; rows the row budget left unfilled keep
+// the label 0xff).  R = rows handed out.
+bcc_status queue_population(bcc_ctx* ctx, bcc_robot robot, const float* edges, int E, int resolution, int min_items,
+                            bcc::PipelineArgs& a, int& R) {
+    const int dof = bcc_robot_dof(robot);
+    const bcc::RobotOps* ops = bcc::robot_ops((int)robot);
+    if (dof < 0 || !ops) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "unknown robot");
+    if (!edges || E <= 0 || resolution <= 0 || min_items < 0)
+        return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad edges, resolution or queue threshold");
+    BCC_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t eb = sizeof(float) * 2 * (size_t)dof * E;
+    BCC_CUDA(ctx, ctx->edges.ensure(eb));
+    BCC_CUDA(ctx, cudaMemcpy(ctx->edges.p, edges, eb, cudaMemcpyHostToDevice));
+    BCC_CUDA(ctx, ctx->results.ensure((size_t)E * ctx->num_envs));
+    bcc_status s = prepare(ctx, robot, ctx->edges.as<float>(), E, resolution, ctx->results.as<uint8_t>(), nullptr, st, a);
+    if (s != BCC_OK) return s;
+    if ((s = ensure_env_code(ctx, st)) != BCC_OK) return s;
+    if ((s = prepare_learned(ctx, a, 0)) != BCC_OK) return s;
+    bcc::MlpState& m = ctx->mlp;
+    BCC_CUDA(ctx, m.lab.ensure((size_t)a.row_cap * bcc::kSegment));
+    BCC_CUDA(ctx, m.y.ensure((size_t)a.row_cap));
+    BCC_CUDA(ctx, cudaMemsetAsync(m.y.p, 0xff, (size_t)a.row_cap, st));
+    a.queue_min_items = min_items;
+    BCC_CUDA(ctx, cudaMemsetAsync(a.q_head, 0, sizeof(unsigned long long), st));
+    BCC_CUDA(ctx, ops->prep(a, st));
+    a.mode = 1;
+    BCC_CUDA(ctx, ops->check_mode(a, st));
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    BCC_CUDA(ctx, ops->queue_features(a, ctx->env_code.as<float>(), m.x.as<uint16_t>(), 16 * std::max(sms, 1), st));
+    BCC_CUDA(ctx, ops->queue_labels(a, m.lab.as<uint8_t>(), m.y.as<uint8_t>(), 16 * std::max(sms, 1), st));
+    unsigned long long head = 0;
+    BCC_CUDA(ctx, cudaMemcpyAsync(&head, a.q_head, sizeof(head), cudaMemcpyDeviceToHost, st));
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    R = (int)std::min<long long>((long long)(uint32_t)head, a.row_cap);
+    return BCC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+bcc_status bcc_mlp_train_queued(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges,
+                                int32_t resolution, int32_t queue_min_items, int64_t num_samples, int32_t epochs,
+                                int32_t batch, float lr, uint64_t seed, float* h_epoch_loss,
+                                float* h_positive_fraction, int64_t* h_rows) {
+    if (!ctx) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs <= 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (num_samples <= 0 || epochs <= 0 || batch < 128)
+        return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad training arguments");
+    if (!ctx->mlp.ready) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "set initial MLP parameters first");
+    bcc::PipelineArgs a;
+    int R = 0;
+    bcc_status s = queue_population(ctx, robot, edges, num_edges, resolution, queue_min_items, a, R);
+    if (s != BCC_OK) return s;
+    bcc::MlpState& m = ctx->mlp;
+    // Seeded shuffle of the filled rows (label 0 or 1), at most num_samples of them.
+    std::vector<uint8_t> yy((size_t)R);
+    if (R > 0) BCC_CUDA(ctx, cudaMemcpy(yy.data(), m.y.p, yy.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> idx;
+    idx.reserve(yy.size());
+    for (int i = 0; i < R; ++i)
+        if (yy[i] <= 1) idx.push_back(i);
+    std::mt19937_64 rng(seed);
+    std::shuffle(idx.begin(), idx.end(), rng);
+    if ((int64_t)idx.size() > num_samples) idx.resize((size_t)num_samples);
+    const int used = (int)idx.size();
+    if (h_rows) *h_rows = used;
+    if (used < batch) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "the queued population has fewer rows than one batch");
+    size_t pos = 0;
+    for (int i : idx) pos += yy[i];
+    if (h_positive_fraction) *h_positive_fraction = (float)((double)pos / used);
+    BCC_CUDA(ctx, m.perm.ensure(sizeof(int) * (size_t)used));
+    BCC_CUDA(ctx, m.x2.ensure(sizeof(uint16_t) * bcc::kMlpIn * (size_t)used));
+    BCC_CUDA(ctx, m.y2.ensure((size_t)used));
+    BCC_CUDA(ctx, cudaMemcpy(m.perm.p, idx.data(), sizeof(int) * (size_t)used, cudaMemcpyHostToDevice));
+    BCC_CUDA(ctx, bcc::launch_gather_rows(m.x.as<uint16_t>(), m.y.as<uint8_t>(), m.perm.as<int>(), used,
+                                          m.x2.as<uint16_t>(), m.y2.as<uint8_t>(), ctx->stream));
+    const long long nb = used / batch;
+    for (int ep = 0; ep < epochs; ++ep) {
+        double tot = 0.0;
+        for (long long b = 0; b < nb; ++b) {
+            float loss = 0.0f;
+            s = bcc_mlp_train_step(ctx, m.x2.as<uint16_t>() + (size_t)b * batch * bcc::kMlpIn,
+                                   m.y2.as<uint8_t>() + (size_t)b * batch, batch, lr, &loss);
+            if (s != BCC_OK) return s;
+            tot += loss;
+        }
+        if (h_epoch_loss) h_epoch_loss[ep] = (float)(tot / (double)(nb * batch));
+    }
+    return BCC_OK;
+}
+
+bcc_status bcc_mlp_rank_metrics(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges,
+                                int32_t resolution, int32_t queue_min_items, double* h_metrics,
+                                int32_t max_metrics) {
+    if (!ctx || !h_metrics || max_metrics < 0) return BCC_ERR_INVALID_ARGUMENT;
+    if (ctx->num_envs <= 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
+    if (!ctx->mlp.ready) return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "learned order needs MLP parameters");
+    bcc::PipelineArgs a;
+    int R = 0;
+    bcc_status s = queue_population(ctx, robot, edges, num_edges, resolution, queue_min_items, a, R);
+    if (s != BCC_OK) return s;
+    bcc::MlpState& m = ctx->mlp;
+    cudaStream_t st = ctx->stream;
+    BCC_CUDA(ctx, m.logits.ensure(sizeof(float) * (size_t)std::max(R, 1)));
+    s = bcc_mlp_forward(ctx, m.x.p, R, m.logits.as<float>(), st);
+    if (s != BCC_OK) return s;
+    BCC_CUDA(ctx, cudaStreamSynchronize(st));
+    unsigned long long head = 0;
+    BCC_CUDA(ctx, cudaMemcpy(&head, a.q_head, sizeof(head), cudaMemcpyDeviceToHost));
+    const int entries = (int)std::min<long long>((long long)(head >> 32), a.q_cap);
+    std::vector<int2> qp((size_t)entries);
+    std::vector<int> qr((size_t)entries), steps((size_t)num_edges);
+    std::vector<float> z((size_t)R);
+    std::vector<uint8_t> lab((size_t)R * bcc::kSegment);
+    if (entries > 0) {
+        BCC_CUDA(ctx, cudaMemcpy(qp.data(), a.q_pairs, sizeof(int2) * qp.size(), cudaMemcpyDeviceToHost));
+        BCC_CUDA(ctx, cudaMemcpy(qr.data(), a.q_rows, sizeof(int) * qr.size(), cudaMemcpyDeviceToHost));
+    }
+    BCC_CUDA(ctx, cudaMemcpy(steps.data(), a.steps, sizeof(int) * steps.size(), cudaMemcpyDeviceToHost));
+    if (R > 0) {
+        BCC_CUDA(ctx, cudaMemcpy(z.data(), m.logits.p, sizeof(float) * z.size(), cudaMemcpyDeviceToHost));
+        BCC_CUDA(ctx, cudaMemcpy(lab.data(), m.lab.p, lab.size(), cudaMemcpyDeviceToHost));
+    }
+    // Per queued pair: sample ranks the walk after the probe takes until its
+    // first hit (all of them for a collision-free pair) in the plain order
+    // (reference ranks 1, 2, ...), the learned order (segments by descending
+    // score, ties by index, each from its last sample; the probed sample 0 is
+    // walked again) and a perfect order (the first colliding sample first).
+    double pairs = 0, coll = 0, rows = 0, pos = 0, wrong = 0;
+    double w_plain = 0, w_learn = 0, w_perf = 0, c_plain = 0, c_learn = 0, c_perf = 0;
+    std::vector<std::pair<float, uint8_t>> scored;
+    scored.reserve((size_t)R);
+    for (int i = 0; i < entries; ++i) {
+        const int ro = qr[i];
+        if (ro < 0) continue;
+        const int n = steps[qp[i].x];
+        const int S = bcc::kLanes * n, nseg = S / bcc::kSegment;
+        if (ro + nseg > R) continue;
+        const uint8_t* L = lab.data() + (size_t)ro * bcc::kSegment;
+        pairs += 1;
+        for (int j = 0; j < nseg; ++j) {
+            const uint8_t yj = L[j * bcc::kSegment + bcc::kSegment - 1];
+            scored.emplace_back(z[ro + j], yj);
+            rows += 1;
+            pos += yj;
+            wrong += ((z[ro + j] > 0.0f) != (yj != 0)) ? 1 : 0;
+        }
+        int r_plain = -1;  // reference rank r -> sample (r % 32) * n + r / 32
+        for (int r = 1; r < S && r_plain < 0; ++r)
+            if (L[(r & 31) * n + (r >> 5)]) r_plain = r;
+        std::vector<int> order((size_t)nseg);
+        for (int j = 0; j < nseg; ++j) order[j] = j;
+        std::stable_sort(order.begin(), order.end(), [&](int u, int v) {
+            const float zu = std::isnan(z[ro + u]) ? -INFINITY : z[ro + u];
+            const float zv = std::isnan(z[ro + v]) ? -INFINITY : z[ro + v];
+            return zu > zv;
+        });
+        int r_learn = -1;
+        for (int p = 0; p < S && r_learn < 0; ++p) {
+            const int k = order[p / bcc::kSegment] * bcc::kSegment + (bcc::kSegment - 1 - p % bcc::kSegment);
+            if (L[k]) r_learn = p + 1;
+        }
+        if (r_plain > 0) {
+            coll += 1;
+            c_plain += r_plain;
+            c_learn += r_learn;
+            c_perf += 1;
+            w_plain += r_plain;
+            w_learn += r_learn;
+            w_perf += 1;
+        } else {
+            w_plain += S - 1;
+            w_learn += S;
+            w_perf += S - 1;
+        }
+    }
+    // AUC of the segment scores against the scored samples' labels (ties half).
+    std::sort(scored.begin(), scored.end(), [](const auto& u, const auto& v) { return u.first < v.first; });
+    double rank_sum = 0, npos = 0;
+    for (size_t i = 0; i < scored.size();) {
+        size_t j = i;
+        while (j < scored.size() && scored[j].first == scored[i].first) ++j;
+        const double avg = 0.5 * (double)(i + 1 + j);
+        for (size_t k = i; k < j; ++k)
+            if (scored[k].second) {
+                rank_sum += avg;
+                npos += 1;
+            }
+        i = j;
+    }
+    const double nneg = (double)scored.size() - npos;
+    const double auc = npos > 0 && nneg > 0 ? (rank_sum - npos * (npos + 1) / 2) / (npos * nneg) : NAN;
+    const double cp = std::max(coll, 1.0), qp_n = std::max(pairs, 1.0);
+    const double metrics[13] = {pairs, rows, coll / qp_n, rows > 0 ? pos / rows : NAN, auc,
+                                c_plain / cp, c_learn / cp, c_perf / cp,
+                                w_plain / qp_n, w_learn / qp_n, w_perf / qp_n,
+                                c_plain > c_perf ? (c_plain - c_learn) / (c_plain - c_perf) : NAN,
+                                rows > 0 ? wrong / rows : NAN};
+    for (int i = 0; i < std::min<int>(max_metrics, 13); ++i) h_metrics[i] = metrics[i];
+    return BCC_OK;
+}
+
 bcc_status bcc_env_code(bcc_ctx* ctx, float* h_code, int32_t num_envs) {
     if (!ctx || !h_code) return BCC_ERR_INVALID_ARGUMENT;
     if (ctx->num_envs < 0) return fail(ctx, BCC_ERR_NO_ENVS, "no environments uploaded");
@@ -803,6 +1130,7 @@ bcc_status bcc_env_code(bcc_ctx* ctx, float* h_code, int32_t num_envs) {
 }
 
 int64_t bcc_last_learned_rows(const bcc_ctx* ctx) {
+    if (ctx && ctx->last_learned_inline) return ctx->last_inline_rows;
     if (!ctx || !ctx->learned_rows_dev) return -1;
     int rows = 0;
     if (cudaMemcpy(&rows, ctx->learned_rows_dev, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
@@ -810,32 +1138,43 @@ int64_t bcc_last_learned_rows(const bcc_ctx* ctx) {
 }
 
 int64_t bcc_last_learned_pairs(const bcc_ctx* ctx) {
+    if (ctx && ctx->last_learned_inline) return 0;  // the inline order queues nothing
     if (!ctx || !ctx->learned_rows_dev) return -1;
     unsigned long long head = 0;  // entries << 32 | rows
     if (cudaMemcpy(&head, ctx->learned_rows_dev, sizeof(head), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     return std::min<int64_t>((int64_t)(head >> 32), ctx->learned_q_cap);
 }
 
-// Launch configuration: [0] edges per CTA, [1] warps per CTA, [2] persistent
-// kernel (0/1), [3] learned-order queue threshold (items).
+// Launch configuration (BCC_LAUNCH_CONFIG_LEN values): [0] edges per CTA,
+// [1] warps per CTA, [2] persistent kernel (0/1), [3] learned-order queue
+// threshold (items), [4] learned-order finish: 1 = each queued pair split over
+// a CTA's warps, 0 = one warp per pair, [5] learned order: 0 = inline, 1 =
+// queued, [6] inline learned order: environment clusters (1..64).
 bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg) {
     if (!ctx || !cfg) return BCC_ERR_INVALID_ARGUMENT;
     cfg[0] = ctx->tune.edges_per_cta;
     cfg[1] = ctx->tune.warps;
     cfg[2] = ctx->tune.persistent;
     cfg[3] = ctx->tune.queue_min_items;
+    cfg[4] = ctx->tune.finish_split;
+    cfg[5] = ctx->tune.learned_mode;
+    cfg[6] = ctx->tune.clusters;
     return BCC_OK;
 }
 
 bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg) {
     if (!ctx || !cfg) return BCC_ERR_INVALID_ARGUMENT;
     if (cfg[0] < 1 || cfg[0] > 4096 || (cfg[1] != 1 && cfg[1] != 2 && cfg[1] != 4 && cfg[1] != 8) ||
-        (cfg[2] != 0 && cfg[2] != 1) || cfg[3] < 0)
+        (cfg[2] != 0 && cfg[2] != 1) || cfg[3] < 0 || (cfg[4] != 0 && cfg[4] != 1) ||
+        (cfg[5] != 0 && cfg[5] != 1) || cfg[6] < 1 || cfg[6] > 64)
         return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad launch configuration");
     ctx->tune.edges_per_cta = cfg[0];
     ctx->tune.warps = cfg[1];
     ctx->tune.persistent = cfg[2];
     ctx->tune.queue_min_items = cfg[3];
+    ctx->tune.finish_split = cfg[4];
+    ctx->tune.learned_mode = cfg[5];
+    ctx->tune.clusters = cfg[6];
     return BCC_OK;
 }
 
@@ -916,19 +1255,47 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
     const bool learned = order == BCC_ORDER_LEARNED && ctx->mlp.ready;
     const int tiles[4] = {32, 64, 128, 256};
     const int warps[2] = {4, 8};
-    const int qmins[6] = {128, 256, 512, 1024, 2048, 4096};
+    const int qmins[7] = {64, 128, 256, 512, 1024, 2048, 4096};
     const bcc::Tune base = best;
-    for (int qi = 0; qi < (learned ? 6 : 1) && s == BCC_OK; ++qi)
+    // Launch shape first (for the learned order at a middle threshold with
+    // one-warp finishes), then the learned order's threshold x finish mode at
+    // that shape, then the shape once more at the chosen threshold and mode.
+    auto sweep_shape = [&](const bcc::Tune& from) {
         for (int ti = 0; ti < 4 && s == BCC_OK; ++ti)
             for (int wi = 0; wi < 2 && s == BCC_OK; ++wi)
                 for (int pe = 0; pe < 2 && s == BCC_OK; ++pe) {
-                    bcc::Tune t = base;
+                    bcc::Tune t = from;
                     t.edges_per_cta = tiles[ti];
                     t.warps = warps[wi];
                     t.persistent = pe;
-                    if (learned) t.queue_min_items = qmins[qi];
                     keep(t);
                 }
+    };
+    bcc::Tune start = base;
+    if (learned) {  // the inline order at 8 clusters while the shape is swept
+        start.learned_mode = 0;
+        start.clusters = 8;
+    }
+    sweep_shape(start);
+    if (learned) {
+        const bcc::Tune shape = best;
+        const int ks[4] = {1, 4, 8, 16};
+        for (int ki = 0; ki < 4 && s == BCC_OK; ++ki) {  // inline order: clusters
+            bcc::Tune t = shape;
+            t.learned_mode = 0;
+            t.clusters = ks[ki];
+            keep(t);
+        }
+        for (int qi = 0; qi < 7 && s == BCC_OK; ++qi)  // queued order: threshold x finish mode
+            for (int sp = 0; sp < 2 && s == BCC_OK; ++sp) {
+                bcc::Tune t = shape;
+                t.learned_mode = 1;
+                t.queue_min_items = qmins[qi];
+                t.finish_split = sp;
+                keep(t);
+            }
+        sweep_shape(best);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ctx->profiling = saved_prof;

@@ -39,6 +39,8 @@ struct MlpState {
     DevBuf images;           // BF16 core-matrix images of W1^T, W2^T, W3^T
     DevBuf acts;             // training activations
     DevBuf x, y, logits;     // per-call inputs / outputs
+    DevBuf lab;              // learned-order population: per-sample verdicts (8 per row)
+    DevBuf x2, y2, perm;     // shuffled training rows and their permutation
     long long step = 0;      // Adam step count
 };
 
@@ -48,6 +50,9 @@ struct Tune {
     int warps = 8;
     int persistent = 1;
     int queue_min_items = 128;
+    int finish_split = 0;    // learned order, queued: 1 = split each queued pair over a CTA's warps
+    int learned_mode = 0;    // learned order: 0 = inline (per-cluster scores), 1 = queued (per-pair scores)
+    int clusters = 8;        // learned order, inline: environment clusters scored per edge
     bool tuned = false;
 };
 
@@ -93,9 +98,16 @@ struct bcc_ctx {
     bcc::DevBuf grid_bounds; // [3][kGridSlabs + 1] slab boundaries of the uploaded set's cull grid
     bcc::DevBuf env_code;    // [num_envs][32] environment encodings
     bool env_code_ready = false;
+    // inline learned order: environment clusters (k-means over the codes)
+    bcc::DevBuf env_cluster; // [num_envs] cluster id
+    bcc::DevBuf centroids;   // [K][32] cluster centroid codes
+    int cluster_k = 0;       // K of the current clustering, 0 = none
+    bcc::DevBuf perms;       // [K][edges][32] per-check lane-block permutations
     bcc::DevBuf q_head, q_pairs, q_rows;   // learned-order queue of undecided pairs
     const int* learned_rows_dev = nullptr; // queue head of the last learned check (entries << 32 | rows)
     int learned_row_cap = 0;
+    bool last_learned_inline = false;      // the last learned check used the inline order
+    long long last_inline_rows = 0;        // its (cluster, segment) rows
     int learned_q_cap = 0;
     bcc::Tune tune;                        // launch configuration (autotuned or default)
     bcc::DevBuf work_counter;              // persistent-kernel work queue head

@@ -158,4 +158,26 @@ cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int nu
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ training rows
+__global__ void gather_rows_kernel(const uint4* __restrict__ x, const uint8_t* __restrict__ y,
+                                   const int* __restrict__ perm, int rows, uint4* __restrict__ x2,
+                                   uint8_t* __restrict__ y2) {
+    constexpr int W = kMlpIn * 2 / 16;  // uint4 words per row
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const int src = perm[i];
+#pragma unroll
+    for (int w = 0; w < W; ++w) x2[(size_t)i * W + w] = x[(size_t)src * W + w];
+    y2[i] = y[src];
+}
+
+cudaError_t launch_gather_rows(const uint16_t* x, const uint8_t* y, const int* perm, int rows, uint16_t* x2,
+                               uint8_t* y2, cudaStream_t st) {
+    static_assert(kMlpIn * 2 % 16 == 0, "feature rows are whole 16-byte words");
+    if (rows <= 0) return cudaSuccess;
+    gather_rows_kernel<<<(rows + 255) / 256, 256, 0, st>>>(reinterpret_cast<const uint4*>(x), y, perm, rows,
+                                                           reinterpret_cast<uint4*>(x2), y2);
+    return cudaGetLastError();
+}
+
 }  // namespace bcc

@@ -46,12 +46,18 @@ struct CheckParams {
     const float* logits;     // [row_cap] segment scores (finish)
     int queue_min_items;     // probe: queue only pairs with at least this many items left
     int* finish_counter;     // next queue entry for the finish kernel
+    int finish_split;        // 1: each queued pair split over a CTA's warps, 0: one warp per pair
     int persistent;          // 1: persistent kernel pulling work items from work_counter
     int* work_counter;
+    // Inline learned order (mode 4): per (cluster, edge) segment permutations.
+    const int* env_cluster;  // [num_envs] cluster of each environment
+    const uint8_t* perms;    // [K][num_edges][32] lane block at each rank of a round
+    int total_segs;          // offs[E] / kSegment
 };
 
 // Samples per learned-order segment: the MLP scores each run of 8 consecutive
-// samples at its middle sample; an edge with step count n has 4 n segments.
+// samples at its last sample, where the walk of the segment starts; an edge
+// with step count n has 4 n segments.
 constexpr int kSegment = 8;
 constexpr int kMaxSegments = 64;  // edges with more segments keep the plain order
 
@@ -84,7 +90,8 @@ struct PipelineArgs {
     int* error_flag;
     cudaEvent_t* stage_events;  // null, or 6 events bracketing the 5 stages
     unsigned long long* counters;
-    int mode;                // 0 plain, 1 probe (rank 0, queue the rest), 2 finish (learned order)
+    int mode;                // 0 plain, 1 probe (rank 0, queue the rest), 2 finish (learned order),
+                             // 4 inline learned order
     unsigned long long* q_head;
     int2* q_pairs;
     int* q_rows;
@@ -93,8 +100,12 @@ struct PipelineArgs {
     const float* logits;
     int queue_min_items;
     int* finish_counter;
+    int finish_split;
     int persistent;
     int* work_counter;
+    const int* env_cluster;
+    const uint8_t* perms;
+    int total_segs;
 };
 
 // Environment check from host-packed records (bcc_pack_envs format), exact
@@ -148,6 +159,14 @@ struct RobotOps {
     cudaError_t (*training_rows)(const PipelineArgs& a, const float* env_code, long long rows,
                                  unsigned long long seed, uint16_t* x, uint8_t* y, cudaStream_t st);
     cudaError_t (*check_records)(RecordsParams P, cudaStream_t st);
+    // Learned-order population: per-sample environment verdicts of the queued
+    // pairs (lab, 8 per MLP row) and of each segment's scored sample (y).
+    cudaError_t (*queue_labels)(const PipelineArgs& a, uint8_t* lab, uint8_t* y, int grid, cudaStream_t st);
+    // Inline learned order: MLP feature rows of every (cluster, segment) and,
+    // from their scores (a.logits), the per-(cluster, edge) 32-block permutations.
+    cudaError_t (*cluster_features)(const PipelineArgs& a, const float* centroids, int K, uint16_t* x,
+                                    cudaStream_t st);
+    cudaError_t (*cluster_perms)(const PipelineArgs& a, int K, uint8_t* perms, cudaStream_t st);
 };
 
 // null for a robot this library was not built with.
@@ -156,6 +175,9 @@ const RobotOps* robot_ops(int robot);
 // Robot-independent kernels (bcc_kernels.cu).
 cudaError_t launch_scan(const int* steps, int E, int* offs, cudaStream_t st);
 cudaError_t launch_env_encode(const float4* blobs, const float4* env_hdr, int num_envs, float* code, cudaStream_t st);
+// Row gather for training: x2[i] = x[perm[i]] (kMlpIn BF16 values), y2[i] = y[perm[i]].
+cudaError_t launch_gather_rows(const uint16_t* x, const uint8_t* y, const int* perm, int rows, uint16_t* x2,
+                               uint8_t* y2, cudaStream_t st);
 size_t check_smem_bytes(int max_prims, int groups, size_t blob_smem, int warps);
 size_t records_smem_bytes(int max_prims, int groups, int warps);
 
@@ -185,8 +207,12 @@ inline CheckParams params_of(const PipelineArgs& a) {
     P.logits = a.logits;
     P.queue_min_items = a.queue_min_items;
     P.finish_counter = a.finish_counter;
+    P.finish_split = a.finish_split;
     P.persistent = a.persistent;
     P.work_counter = a.work_counter;
+    P.env_cluster = a.env_cluster;
+    P.perms = a.perms;
+    P.total_segs = a.total_segs;
     return P;
 }
 

@@ -36,34 +36,53 @@ constexpr int kOffW4 = kOffB3 + kMlpHidden;
 constexpr int kOffB4 = kOffW4 + kMlpHidden;
 static_assert(kOffB4 + 1 == kMlpParams, "parameter layout");
 
-// Shared-memory map of the forward kernel (bytes): the weight images, then per
-// row group its X tile (128 x 48) and H tile (128 x 128), the bias vectors, the
-// groups' mbarriers and the TMEM address slot.
+// Images (BF16 core-matrix layouts, bcc_tc.cuh): W1^T [128][48] -- its column
+// 47 carries b1, the forward kernel reads feature 47 as 1 --, W2^T, W3^T
+// [128][128] (the training kernel uses these three), then for the forward
+// kernel only: W4 [16][128] (row 0 = w4, the last layer as an N = 16 MMA) and
+// B2, B3 [128][16] (column 0 = b2 / b3, added by one K = 16 MMA against a
+// ones column).
 constexpr uint32_t kImgW1 = kMlpHidden * kMlpIn * 2;       // 12288
 constexpr uint32_t kImgW = kMlpHidden * kMlpHidden * 2;    // 32768
+constexpr uint32_t kImgSmall = kMlpHidden * 16 * 2;         // 4096: W4, B2, B3 and the ones image
+constexpr uint32_t kImagesW = kImgW1 + 2 * kImgW;           // W1T | W2T | W3T
+constexpr uint32_t kImagesBytes = kImagesW + 3 * kImgSmall;  // ... | W4 | B2 | B3
+constexpr int kBiasCol = kMlpIn - 1;                        // feature 47: reserved, read as 1 by the forward kernel
+
+// Shared-memory map of the forward kernel (bytes): the images, the ones image
+// (A operand of the bias MMAs), then per row group its X tile (128 x 48) and H
+// tile (128 x 128), b4, the groups' mbarriers and the TMEM address slot.
 constexpr uint32_t kSmW1 = 0;
 constexpr uint32_t kSmW2 = kSmW1 + kImgW1;
 constexpr uint32_t kSmW3 = kSmW2 + kImgW;
+constexpr uint32_t kSmW4 = kSmW3 + kImgW;
+constexpr uint32_t kSmB2 = kSmW4 + kImgSmall;
+constexpr uint32_t kSmB3 = kSmB2 + kImgSmall;
+constexpr uint32_t kSmOnes = kSmB3 + kImgSmall;
 constexpr int kFwdGroups = 3;                              // independent 128-row tile streams per CTA
 constexpr uint32_t kFwdTmemCols = 512;                     // power of two >= 128 x groups
-constexpr uint32_t kSmGroup0 = kSmW3 + kImgW;              // group g: X at +g*stride, H at +kImgW1
+constexpr uint32_t kSmGroup0 = kSmOnes + kImgSmall;        // group g: X at +g*stride, H at +kImgW1
 constexpr uint32_t kSmGroupStride = kImgW1 + kImgW;
-constexpr uint32_t kSmVec = kSmGroup0 + kFwdGroups * kSmGroupStride;  // b1 b2 b3 w4 (4 x 128) + b4
-constexpr uint32_t kSmBar = kSmVec + 4 * kMlpHidden * 4 + 16;
+constexpr uint32_t kSmVec = kSmGroup0 + kFwdGroups * kSmGroupStride;  // b4
+constexpr uint32_t kSmBar = kSmVec + 16;
 constexpr uint32_t kSmTmem = kSmBar + 8 * kFwdGroups;
 constexpr uint32_t kFwdSmem = kSmTmem + 8;
-constexpr uint32_t kImagesBytes = kImgW1 + 2 * kImgW;       // W1T | W2T | W3T
 static_assert(kSmGroup0 % 16 == 0 && kSmGroupStride % 16 == 0, "core-matrix images are 16-byte aligned");
+static_assert(kSmW4 == kImagesW && kSmOnes == kImagesBytes, "forward images are copied as one block");
 static_assert(kFwdSmem <= 227 * 1024, "forward kernel shared memory");
 
 // ---------------------------------------------------------------- images
 // FP32 masters -> BF16 core-matrix images of W1^T [128][48], W2^T, W3^T.
+// Feature 47 is zero in every input row, so W1's row 47 never contributes;
+// the image's column 47 holds b1 instead, which the forward kernel adds by
+// reading feature 47 as 1 (the training kernel reads it as the 0 it is and
+// adds b1 in its epilogue).
 __global__ void mlp_pack_kernel(const float* __restrict__ params, uint8_t* __restrict__ images) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n1 = kMlpHidden * kMlpIn, n2 = kMlpHidden * kMlpHidden;
+    const int n1 = kMlpHidden * kMlpIn, n2 = kMlpHidden * kMlpHidden, ns = kMlpHidden * 16;
     if (i < n1) {
         const int out = i / kMlpIn, in = i % kMlpIn;
-        const float w = params[kOffW1 + in * kMlpHidden + out];
+        const float w = in == kBiasCol ? params[kOffB1 + out] : params[kOffW1 + in * kMlpHidden + out];
         *reinterpret_cast<__nv_bfloat16*>(images + tc::cm_offset(out, in, kMlpIn)) = __float2bfloat16_rn(w);
     } else if (i < n1 + 2 * n2) {
         const int j = i - n1;
@@ -72,10 +91,52 @@ __global__ void mlp_pack_kernel(const float* __restrict__ params, uint8_t* __res
         const float w = params[(layer ? kOffW3 : kOffW2) + in * kMlpHidden + out];
         *reinterpret_cast<__nv_bfloat16*>(images + kImgW1 + layer * kImgW + tc::cm_offset(out, in, kMlpHidden)) =
             __float2bfloat16_rn(w);
+    } else if (i < n1 + 2 * n2 + ns) {  // W4 [16][128]: row 0 = w4
+        const int j = i - n1 - 2 * n2;
+        const int out = j / kMlpHidden, in = j % kMlpHidden;
+        const float w = out == 0 ? params[kOffW4 + in] : 0.0f;
+        *reinterpret_cast<__nv_bfloat16*>(images + kImagesW + tc::cm_offset(out, in, kMlpHidden)) =
+            __float2bfloat16_rn(w);
+    } else if (i < n1 + 2 * n2 + 3 * ns) {  // B2, B3 [128][16]: column 0 = bias
+        const int j = i - n1 - 2 * n2 - ns;
+        const int layer = j / ns, r = j % ns;
+        const int out = r / 16, in = r % 16;
+        const float w = in == 0 ? params[(layer ? kOffB3 : kOffB2) + out] : 0.0f;
+        *reinterpret_cast<__nv_bfloat16*>(images + kImagesW + (1 + layer) * kImgSmall + tc::cm_offset(out, in, 16)) =
+            __float2bfloat16_rn(w);
     }
 }
 
 // ---------------------------------------------------------------- forward
+// ReLU of two FP32 values, rounded to BF16 and packed (lo in the low half).
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
+// Forward epilogue of a hidden layer whose bias the MMAs already added: this
+// thread's accumulator row, ReLU, BF16 into the H image (one conversion per
+// two values).  Two 16-column loads are in flight before each wait.
+__device__ __forceinline__ void epilogue_relu_only(uint32_t taddr, uint8_t* himg, int row) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
+        float v[32];
+        tc::tmem_ld16(taddr + c0, v);
+        tc::tmem_ld16(taddr + c0 + 16, v + 16);
+        tc::wait_ld();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint4 w;
+            w.x = relu_bf16x2(v[8 * q + 0], v[8 * q + 1]);
+            w.y = relu_bf16x2(v[8 * q + 2], v[8 * q + 3]);
+            w.z = relu_bf16x2(v[8 * q + 4], v[8 * q + 5]);
+            w.w = relu_bf16x2(v[8 * q + 6], v[8 * q + 7]);
+            *reinterpret_cast<uint4*>(himg + tc::cm_offset(row, c0 + 8 * q, kMlpHidden)) = w;
+        }
+    }
+}
+
 // Bias + ReLU of one 128-column accumulator row (this thread's row), written as
 // BF16 into the H image; `taddr` = TMEM address of column 0 of this warp's lanes.
 // One warp group's epilogue of a hidden layer: TMEM accumulator row + bias, ReLU,
@@ -127,9 +188,11 @@ __device__ __forceinline__ bool group_sync_or(bool pred, int grp) {
 // Persistent: each CTA loads the weights once; its three warp groups (4 warps,
 // one row per thread each) run independent streams of 128-row tiles, each with
 // its own X/H images, TMEM accumulator (columns 128 g ..) and mbarrier, so one
-// group's MMAs overlap the others' epilogues (three groups measured 1.3x two:
-// the epilogues, not the MMAs, set the pace).  x: BF16 [rows][48] row-major;
-// logits: FP32 [rows].
+// group's MMAs overlap the others' epilogues.  The biases ride in the MMAs (b1
+// as column 47 of W1^T against feature 47 read as 1; b2, b3 by a K = 16 MMA of
+// a ones column against B2 / B3) and the output layer is an N = 16 MMA against
+// W4, so each hidden epilogue is only ReLU + BF16 conversion + store.  x: BF16
+// [rows][48] row-major (feature 47 zero); logits: FP32 [rows].
 __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     mlp_forward_kernel(const uint16_t* __restrict__ x, int rows, const int* __restrict__ rows_dev,
                        const uint4* __restrict__ images, const float* __restrict__ params, float* __restrict__ logits,
@@ -148,14 +211,12 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     uint8_t* hs = xs + kImgW1;
 
     for (uint32_t i = t; i < kImagesBytes / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
-    for (int i = t; i < kMlpHidden; i += blockDim.x) {
-        vec[i] = params[kOffB1 + i];
-        vec[kMlpHidden + i] = params[kOffB2 + i];
-        vec[2 * kMlpHidden + i] = params[kOffB3 + i];
-        vec[3 * kMlpHidden + i] = params[kOffW4 + i];
+    if (t < 128) {  // ones image [128][16]: column 0 = 1 (BF16 0x3f80), the rest 0
+        *reinterpret_cast<uint4*>(sm + kSmOnes + tc::cm_offset(t, 0, 16)) = make_uint4(0x3f80u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(sm + kSmOnes + tc::cm_offset(t, 8, 16)) = make_uint4(0u, 0u, 0u, 0u);
     }
     if (t == 0) {
-        vec[4 * kMlpHidden] = params[kOffB4];
+        vec[0] = params[kOffB4];
         for (int g = 0; g < kFwdGroups; ++g) mbar_init(reinterpret_cast<uint64_t*>(sm + kSmBar) + g, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -166,14 +227,16 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     const uint32_t tmem = *tmem_slot + 128u * grp;
     const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     const uint32_t idesc = tc::make_idesc_bf16(128, kMlpHidden, 0, 0);
+    const uint32_t idesc16 = tc::make_idesc_bf16(128, 16, 0, 0);
     const uint32_t sbase = tc::smem_addr(sm);
+    const float b4 = vec[0];
     uint32_t phase = 0;
     bool bad = false;
 
     const int tiles = (rows + 127) / 128;
     const int tile_step = gridDim.x * kFwdGroups;
     // X rows are loaded one tile ahead into registers, so their latency overlaps
-    // the current tile's three layers.
+    // the current tile's layers.
     uint4 xv[kMlpIn / 8];
     auto load_x = [&](int tile) {
         const int row = tile * 128 + gt;
@@ -181,28 +244,43 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
 #pragma unroll
         for (int j = 0; j < kMlpIn / 8; ++j) xv[j] = (tile < tiles && row < rows) ? src[j] : make_uint4(0, 0, 0, 0);
     };
+    static_assert(kBiasCol == kMlpIn - 1, "the bias feature is the last of the row's last 16-byte chunk");
     load_x(blockIdx.x * kFwdGroups + grp);
     for (int tile = blockIdx.x * kFwdGroups + grp; tile < tiles && !bad; tile += tile_step) {
         const int row = tile * 128 + gt;
-        // X tile: this thread's row, six 16-byte chunks of 8 features.
+        // X tile: this thread's row, six 16-byte chunks of 8 features; feature 47
+        // (zero in the input) is read as 1 to pick up b1 from W1^T's column 47.
+        xv[kMlpIn / 8 - 1].w = (xv[kMlpIn / 8 - 1].w & 0xffffu) | 0x3f800000u;
 #pragma unroll
         for (int j = 0; j < kMlpIn / 8; ++j) *reinterpret_cast<uint4*>(xs + tc::cm_offset(gt, 8 * j, kMlpIn)) = xv[j];
         load_x(tile + tile_step);
-        // Three layers: MMAs from the group's first thread, epilogue from all.
+        // Four MMA stages (three hidden layers, the output layer): MMAs from the
+        // group's first thread, epilogue from all.
 #pragma unroll 1
-        for (int layer = 0; layer < 3; ++layer) {
+        for (int layer = 0; layer < 4; ++layer) {
             tc::fence_async_smem();
             tc::fence_before();
             group_sync(grp);
             if (gt == 0) {
                 tc::fence_after();
-                const uint32_t a0 = tc::smem_addr(layer == 0 ? xs : hs);
-                const uint32_t b0 = sbase + (layer == 0 ? kSmW1 : layer == 1 ? kSmW2 : kSmW3);
-                const int K = layer == 0 ? kMlpIn : kMlpHidden;
-                const uint32_t sbo = (uint32_t)(K / 8) * 128u;
-                for (int s = 0; s < K / 16; ++s)
-                    tc::mma_bf16(tmem, tc::make_desc(a0 + 256u * s, 128u, sbo), tc::make_desc(b0 + 256u * s, 128u, sbo),
-                                 idesc, s > 0 ? 1u : 0u);
+                if (layer == 0) {
+                    const uint32_t a0 = tc::smem_addr(xs), b0 = sbase + kSmW1;
+                    constexpr uint32_t sbo = (uint32_t)(kMlpIn / 8) * 128u;
+                    for (int s = 0; s < kMlpIn / 16; ++s)
+                        tc::mma_bf16(tmem, tc::make_desc(a0 + 256u * s, 128u, sbo),
+                                     tc::make_desc(b0 + 256u * s, 128u, sbo), idesc, s > 0 ? 1u : 0u);
+                } else {
+                    const uint32_t a0 = tc::smem_addr(hs);
+                    const uint32_t b0 = sbase + (layer == 1 ? kSmW2 : layer == 2 ? kSmW3 : kSmW4);
+                    constexpr uint32_t sbo = (uint32_t)(kMlpHidden / 8) * 128u;
+                    for (int s = 0; s < kMlpHidden / 16; ++s)
+                        tc::mma_bf16(tmem, tc::make_desc(a0 + 256u * s, 128u, sbo),
+                                     tc::make_desc(b0 + 256u * s, 128u, sbo), layer == 3 ? idesc16 : idesc,
+                                     s > 0 ? 1u : 0u);
+                    if (layer < 3)  // + bias: ones [128][16] x B [128][16]^T
+                        tc::mma_bf16(tmem, tc::make_desc(sbase + kSmOnes, 128u, 256u),
+                                     tc::make_desc(sbase + (layer == 1 ? kSmB2 : kSmB3), 128u, 256u), idesc, 1u);
+                }
                 tc::commit(bar);
             }
             const bool ok = mbar_wait_bounded(bar, phase, 1u << 22);
@@ -212,21 +290,12 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
             }
             phase ^= 1u;
             tc::fence_after();
-            if (layer < 2) {
-                epilogue_relu_to_smem(taddr, vec + layer * kMlpHidden, hs, gt);
+            if (layer < 3) {
+                epilogue_relu_only(taddr, hs, gt);
             } else {
-                float acc = vec[4 * kMlpHidden];
-#pragma unroll 1
-                for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
-                    float v[32];
-                    tc::tmem_ld16(taddr + c0, v);
-                    tc::tmem_ld16(taddr + c0 + 16, v + 16);
-                    tc::wait_ld();
-#pragma unroll
-                    for (int i = 0; i < 32; ++i)
-                        acc = fmaf(fmaxf(v[i] + vec[2 * kMlpHidden + c0 + i], 0.0f), vec[3 * kMlpHidden + c0 + i], acc);
-                }
-                if (row < rows) logits[row] = acc;
+                const float z = tc::tmem_ld1(taddr);
+                tc::wait_ld();
+                if (row < rows) logits[row] = z + b4;
             }
         }
     }
@@ -302,7 +371,7 @@ __global__ void __launch_bounds__(128, 1)
     float* gv = reinterpret_cast<float*>(sm + kTrGrad);    // db1 | db2 | db3 | dw4 | db4, loss
     const float inv_rows = 1.0f / (float)rows;
 
-    for (uint32_t i = t; i < kImagesBytes / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
+    for (uint32_t i = t; i < kImagesW / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
     for (int i = t; i < kMlpHidden; i += blockDim.x) {
         vec[i] = params[kOffB1 + i];
         vec[kMlpHidden + i] = params[kOffB2 + i];
@@ -547,7 +616,7 @@ cudaError_t mlp_adam(float* d_params, const float* d_grads, float* d_m, float* d
 }
 
 cudaError_t mlp_pack(const float* d_params, uint8_t* d_images, cudaStream_t st) {
-    const int n = kMlpHidden * kMlpIn + 2 * kMlpHidden * kMlpHidden;
+    const int n = kMlpHidden * kMlpIn + 2 * kMlpHidden * kMlpHidden + 3 * kMlpHidden * 16;
     mlp_pack_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_params, d_images);
     return cudaGetLastError();
 }

@@ -379,6 +379,23 @@ __device__ __forceinline__ bool bound_hits_any(const float4* __restrict__ table,
     return __any_sync(kFull, any);
 }
 
+// Learned order, rank r -> sample index: segments in the order perm gives
+// (descending MLP score), each walked from its last sample back to its first.
+// The MLP scores a segment at its last sample (queue_features_kernel), so the
+// scored sample is the first one checked; a collision that starts inside an
+// edge whose start is free usually extends to the edge's end, so within a
+// segment the later samples are the likelier hits.
+__device__ __forceinline__ int learned_rank_to_sample(const uint8_t* perm, int r) {
+    return (int)perm[r >> 3] * kSegment + (kSegment - 1 - (r & (kSegment - 1)));
+}
+
+// Inline learned order: a permutation pi of the 32 lane blocks (block t =
+// samples t n .. t n + n - 1, the samples the reference's lane t checks) with
+// pi[0] = 0; rank r -> sample pi[r % 32] n + r / 32, so every round visits the
+// blocks in learned order, round 0 first (the reference's coarse sweep,
+// re-prioritised), starting with sample 0 (where most colliding pairs collide).
+// Each lane holds pi[lane]; the walk fetches pi[r % 32] by shuffle.
+
 struct WalkStats {
     unsigned long long chunks = 0, gates = 0, leaf = 0;
 };
@@ -433,6 +450,21 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
     constexpr int G = M::num_env_groups;
     constexpr int GB = group_bits<M>();
     constexpr bool kOver = has_overhang<M>();
+    // rank -> sample: reference order (MODE 0, 1, or no perm), learned order
+    // (MODE 2, 3), inline learned order (MODE 4: perm = the pair's 32-block
+    // permutation, block fetched by a shuffle every lane executes).
+    const int pi = MODE == 4 && perm ? (int)perm[threadIdx.x & 31] : (int)(threadIdx.x & 31);
+    auto block_of = [&](int rr) {
+        if constexpr (MODE == 4) return __shfl_sync(kFull, pi, rr & (kLanes - 1));
+        return rr & (kLanes - 1);
+    };
+    auto sample_of = [&](int rr, int blk) {
+        if constexpr (MODE == 0 || MODE == 1 || MODE == 4) {
+            return blk * n + (rr >> 5);
+        } else {
+            return perm ? learned_rank_to_sample(perm, rr) : reference_rank_to_sample(rr, n);
+        }
+    };
     const int lane = threadIdx.x & 31;
     const int total = kLanes * n * C;
     const int w_last = w_end < 0 ? total : w_end;
@@ -474,8 +506,9 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 const int fc = __shfl_sync(kFull, GL.fc, g);
                 first = fc & 0xffff;
                 const int gcnt = fc >> 16;
+                const int blk = block_of(r);
                 if (w0 + lane < total) {
-                    k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+                    k = sample_of(r, blk);
                     float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
                     bs.w += kEnvInflate;
                     gate = sphere_hits_prim(bs, prim + p * kPrimF4);
@@ -486,8 +519,9 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 // which leaves its longer body the registers it needs (measured faster
                 // for Fetch and Baxter).
                 const DevTables<M>& T = tab<M>();
+                const int blk = block_of(r);
                 if (w0 + lane < total) {
-                    k = perm ? (int)perm[r >> 3] * kSegment + (r & (kSegment - 1)) : reference_rank_to_sample(r, n);
+                    k = sample_of(r, blk);
                     const uint32_t pr = pairs[c];
                     g = (int)(pr & ((1u << GB) - 1u));
                     p = (int)(pr >> GB);
@@ -615,6 +649,30 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
     return collide;
 }
 
+// Learned order, whole warp: perm_buf[rank] = segment, the edge's nseg <= 64
+// segments in descending MLP score (scores[0 .. nseg)), ties by index, NaN
+// last; returns segment 0's rank.
+__device__ __forceinline__ int rank_segments(const float* scores, int nseg, uint8_t* perm_buf) {
+    const int lane = threadIdx.x & 31;
+    float v0 = lane < nseg ? scores[lane] : -INFINITY;
+    float v1 = lane + 32 < nseg ? scores[lane + 32] : -INFINITY;
+    v0 = isnan(v0) ? -INFINITY : v0;
+    v1 = isnan(v1) ? -INFINITY : v1;
+    int rank0 = 0, rank1 = 0;
+    for (int i = 0; i < nseg; ++i) {
+        const float vi = __shfl_sync(kFull, i < 32 ? v0 : v1, i & 31);
+        rank0 += (vi > v0 || (vi == v0 && i < lane)) ? 1 : 0;
+        rank1 += (vi > v1 || (vi == v1 && i < lane + 32)) ? 1 : 0;
+    }
+    if (lane < nseg) perm_buf[rank0] = (uint8_t)lane;
+    if (lane + 32 < nseg) perm_buf[rank1] = (uint8_t)(lane + 32);
+    return __shfl_sync(kFull, rank0, 0);
+}
+
+__device__ __forceinline__ void learned_perm(const CheckParams& P, int seg_row, int nseg, uint8_t* perm_buf) {
+    rank_segments(P.logits + seg_row, nseg, perm_buf);
+}
+
 // Learned-order queue: lane 0 of a probing warp reserves a queue entry and the
 // 4 n MLP rows of the pair's segments with one 64-bit atomic on q_head (entries
 // in the high word, rows in the low word).  Returns the pair's first MLP row,
@@ -636,13 +694,21 @@ __device__ __forceinline__ int queue_pair(const CheckParams& P, int e, int env, 
     return r;
 }
 
+// Inline learned order of pair (env, e): the 32-block permutation scored for
+// the environment's cluster.
+__device__ __forceinline__ const uint8_t* inline_perm(const CheckParams& P, int env, int e) {
+    return P.perms + ((size_t)P.env_cluster[env] * P.num_edges + e) * kLanes;
+}
+
 // One (environment, edge) pair, whole warp: cull, pair-list compaction and the
 // walk.  MODE 0: plain order, full walk.  MODE 1 (learned pipeline, phase 1):
 // plain order; a pair still undecided once rank 0 (its first sample) is walked may be
 // queued (with MLP rows for its segments) instead of getting a verdict.  MODE 2
 // (phase 3): a queued pair (first MLP row seg_row) walked in descending
-// segment score.  `prim` holds the environment's records (shared or global
-// memory), `masks` its cull masks, W 64-bit words per mask.
+// segment score, its chunks split over the CTA's warps; MODE 3 (phase 3, one
+// warp per pair): the same walk by this warp alone, which writes the verdict.
+// `prim` holds the environment's records (shared or global memory), `masks`
+// its cull masks, W 64-bit words per mask.
 template <class M, int MODE>
 __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e, int seg_row, const float4* prim,
                                            const uint64_t* __restrict__ masks, int np, int W, uint16_t* pairs,
@@ -716,20 +782,9 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
         // Learned order: rank the edge's 4 n segments by their MLP score
         // (descending, ties by index; NaN scores last).
         const int nseg = 4 * n;
-        const bool learned = MODE == 2 && seg_row >= 0 && nseg <= kMaxSegments;
+        const bool learned = (MODE == 2 || MODE == 3) && seg_row >= 0 && nseg <= kMaxSegments;
         if (learned) {
-            float v0 = lane < nseg ? P.logits[seg_row + lane] : -INFINITY;
-            float v1 = lane + 32 < nseg ? P.logits[seg_row + lane + 32] : -INFINITY;
-            v0 = isnan(v0) ? -INFINITY : v0;
-            v1 = isnan(v1) ? -INFINITY : v1;
-            int rank0 = 0, rank1 = 0;
-            for (int i = 0; i < nseg; ++i) {
-                const float vi = __shfl_sync(kFull, i < 32 ? v0 : v1, i & 31);
-                rank0 += (vi > v0 || (vi == v0 && i < lane)) ? 1 : 0;
-                rank1 += (vi > v1 || (vi == v1 && i < lane + 32)) ? 1 : 0;
-            }
-            if (lane < nseg) perm_buf[rank0] = (uint8_t)lane;
-            if (lane + 32 < nseg) perm_buf[rank1] = (uint8_t)(lane + 32);
+            learned_perm(P, seg_row, nseg, perm_buf);
             __syncwarp();
         }
         if constexpr (MODE == 1 && !has_overhang<M>()) {
@@ -754,6 +809,9 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
                 collide = walk_pairs<M, 0>(P.table, row0, n, Cs, pairs, prim, np, nullptr, 0, GL, undecided, st,
                                            queue);
             }
+        } else if constexpr (MODE == 4) {
+            collide = walk_pairs<M, 4>(P.table, row0, n, Cs, pairs, prim, np, inline_perm(P, env, e), 0, GL,
+                                       undecided, st, queue);
         } else {
             collide = walk_pairs<M, MODE>(P.table, row0, n, Cs, pairs, prim, np, learned ? perm_buf : nullptr,
                                           P.queue_min_items, GL, undecided, st, queue, 32 * chunk0, -1, stride,
@@ -818,13 +876,167 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
     }
 }
 
+// Pairs whose cull and compaction one warp does together: lanes are grouped G
+// to a pair (Panda 10 -> 3 pairs, Fetch 15 -> 2, Baxter 32 -> 1), so the
+// per-pair set-up -- slab-range loads, mask ANDs, counts, the scan and the
+// list writes -- runs on 30 (or 30, 32) lanes instead of G.
+template <class M>
+constexpr int pairs_per_setup() {
+    return kLanes / M::num_env_groups;
+}
+
+// The walk of one pair whose whole candidate list is in `pairs` (C entries,
+// C <= pairs_per_warp), whole warp, and its verdict: MODE 0 plain order;
+// MODE 1 probe (plain walk of rank 0, then queue the pair or walk on); MODE 4
+// inline learned order.
+template <class M, int MODE>
+__device__ __forceinline__ void walk_listed_pair(const CheckParams& P, int env, int e, int C, const uint16_t* pairs,
+                                                 const float4* prim, int np, const GroupLanes& GL) {
+    const int lane = threadIdx.x & 31;
+    const int n = P.steps[e];
+    const size_t row0 = (size_t)P.offs[e];
+    bool collide = false, undecided = false;
+    WalkStats st;
+    auto queue = [&]() {
+        int ro = -1;
+        if (lane == 0) ro = queue_pair(P, e, env, n);
+        return __shfl_sync(kFull, ro, 0) >= 0;
+    };
+    if constexpr (MODE == 1 && !has_overhang<M>()) {
+        // Probe, as in check_pair: two plain walks split at the chunk that
+        // completes rank 0, the queue decision between them.
+        const int total = kLanes * n * C;
+        const int w_dec = (((C - 1) >> 5) << 5) + 32;
+        if (total - w_dec >= P.queue_min_items) {
+            collide = walk_pairs<M, 0>(P.table, row0, n, C, pairs, prim, np, nullptr, 0, GL, undecided, st, queue, 0,
+                                       w_dec);
+            if (!collide) {
+                if (queue())
+                    undecided = true;
+                else
+                    collide = walk_pairs<M, 0>(P.table, row0, n, C, pairs, prim, np, nullptr, 0, GL, undecided, st,
+                                               queue, w_dec);
+            }
+        } else {
+            collide = walk_pairs<M, 0>(P.table, row0, n, C, pairs, prim, np, nullptr, 0, GL, undecided, st, queue);
+        }
+    } else if constexpr (MODE == 4) {
+        collide = walk_pairs<M, 4>(P.table, row0, n, C, pairs, prim, np, inline_perm(P, env, e), 0, GL, undecided,
+                                   st, queue);
+    } else {
+        collide = walk_pairs<M, MODE>(P.table, row0, n, C, pairs, prim, np, nullptr, P.queue_min_items, GL, undecided,
+                                      st, queue);
+    }
+    if (MODE == 1 && undecided) return;  // queued: the finish pass walks, counts and writes the verdict
+    if (lane == 0) {
+        P.results[(size_t)e * P.num_envs + env] = collide ? 1 : 0;
+        if (P.counters) {
+            atomicAdd(P.counters + 0, 1ull);
+            atomicAdd(P.counters + 1, (unsigned long long)C);
+            atomicAdd(P.counters + 2, st.chunks);
+            atomicAdd(P.counters + 3, st.gates);
+            atomicAdd(P.counters + 4, st.leaf);
+            atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
+        }
+    }
+}
+
+// Pairs (env, e0 .. e0 + count - 1), count <= pairs_per_setup<M>(), whole
+// warp: lane group s = lane / G culls pair s (lane g of the group ANDs link
+// g's three masks), a scan inside each group gives every link its offset,
+// the groups' lists are laid out one after another in `pairs` and written in
+// one pass; then the warp walks the pairs one at a time.  When the lists do
+// not fit the warp's buffer together, each pair goes through check_pair
+// (segments).
+template <class M, int MODE>
+__device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, int e0, int count, const float4* prim,
+                                                 const uint64_t* __restrict__ masks, int np, int W, uint16_t* pairs,
+                                                 const GroupLanes& GL) {
+    constexpr int G = M::num_env_groups;
+    constexpr int GB = group_bits<M>();
+    constexpr int SUB = pairs_per_setup<M>();
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / G;
+    const int g = lane - sub * G;
+    const bool live = sub < count;
+    const int e = e0 + (live ? sub : 0);
+    const int self = live ? P.edge_self[e] : 1;
+    const int code = (live && !self && np > 0) ? P.edge_tri[(size_t)e * G + g] : -1;
+    auto mask_word = [&](int w) {
+        const int tx = code & 1023, ty = (code >> 10) & 1023, tz = code >> 20;
+        return __ldg(masks + tx * W + w) & __ldg(masks + (kGridTri + ty) * W + w) &
+               __ldg(masks + (2 * kGridTri + tz) * W + w);
+    };
+    int cnt = 0;
+    if (code >= 0)
+        for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
+    // inclusive scan inside each group of G lanes
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, inc, o);
+        if (g >= o) inc += y;
+    }
+    // every pair's candidate count and list base
+    int Cs[SUB], base[SUB], total = 0;
+#pragma unroll
+    for (int t = 0; t < SUB; ++t) {
+        Cs[t] = __shfl_sync(kFull, inc, t * G + G - 1);
+        base[t] = total;
+        total += t < count ? Cs[t] : 0;
+    }
+    if (total > P.pairs_per_warp) {
+        for (int t = 0; t < count; ++t)
+            check_pair<M, MODE>(P, env, e0 + t, -1, prim, masks, np, W, pairs, nullptr, GL);
+        return;
+    }
+    if (cnt > 0) {
+        int idx = inc - cnt;
+#pragma unroll
+        for (int t = 0; t < SUB; ++t)
+            if (t == sub) idx += base[t];
+        for (int w = 0; w < W; ++w) {
+            uint64_t m = mask_word(w);
+            while (m) {
+                const int b = __ffsll((long long)m) - 1;
+                pairs[idx++] = (uint16_t)(((w * 64 + b) << GB) | g);
+                m &= m - 1;
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int t = 0; t < count; ++t) {
+        const int et = e0 + t;
+        const int self_t = __shfl_sync(kFull, self, t * G);
+        if (np == 0 || self_t) {  // decided without a walk (not counted as walked, as in check_pair)
+            if (lane == 0) P.results[(size_t)et * P.num_envs + env] = self_t ? 1 : 0;
+            continue;
+        }
+        if (Cs[t] == 0) {  // nothing survives the cull: free
+            if (lane == 0) {
+                P.results[(size_t)et * P.num_envs + env] = 0;
+                if (P.counters) atomicAdd(P.counters + 0, 1ull);
+            }
+            continue;
+        }
+        int bt = 0;
+#pragma unroll
+        for (int u = 0; u < SUB; ++u)
+            if (u == t) bt = base[u];
+        walk_listed_pair<M, MODE>(P, env, et, Cs[t], pairs + bt, prim, np, GL);
+    }
+    __syncwarp();  // every lane is done with the lists before the next group's writes
+}
+
 // check_tile processes the edges of one (environment, edge tile) work item
 // (modes 0 and 1) with the environment's records already staged in shared
 // memory; it is shared by the one-CTA-per-item grid kernel and the persistent
-// kernel.
+// kernel.  Each warp takes pairs_per_setup consecutive edges at a time.
 template <class M, int WARPS, int MODE>
 __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int tile, int n_slots,
                                            const unsigned char* smem, float4 h0, float4 h1) {
+    constexpr int SUB = pairs_per_setup<M>();
     const int e_begin = tile * P.edges_per_cta;
     const int warp = threadIdx.x >> 5;
     const uint32_t shape = __float_as_uint(h1.w);
@@ -838,8 +1050,14 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
     uint16_t* pairs =
         reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) + (size_t)warp * P.pairs_per_warp;
     const GroupLanes GL = group_lanes<M>();
-    for (int slot = warp; slot < n_slots; slot += WARPS)
-        check_pair<M, MODE>(P, env, e_begin + slot, -1, prim, masks, np, W, pairs, nullptr, GL);
+    if constexpr (SUB > 1) {
+        for (int slot = warp * SUB; slot < n_slots; slot += WARPS * SUB)
+            check_pair_group<M, MODE>(P, env, e_begin + slot, min(SUB, n_slots - slot), prim, masks, np, W, pairs,
+                                      GL);
+    } else {
+        for (int slot = warp; slot < n_slots; slot += WARPS)
+            check_pair<M, MODE>(P, env, e_begin + slot, -1, prim, masks, np, W, pairs, nullptr, GL);
+    }
 }
 
 __device__ __forceinline__ int tile_slots(const CheckParams& P, int tile) {
@@ -960,16 +1178,56 @@ constexpr int finish_min_ctas() {
     return (M::check_warps_per_sm < 32 ? M::check_warps_per_sm : 32) / WARPS;
 }
 
+// Learned order, phase 3, one warp per queued pair: each warp pulls entries
+// from finish_counter on its own, culls, ranks the segments and walks the
+// pair in learned order (MODE 3).  No CTA barrier per pair, so many pairs are
+// in flight per SM; a long walk is not split, so the longest queued pair sets
+// the tail.  Compiled like finish_kernel.
 template <class M, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finish_kernel(CheckParams P) {
+__global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finish_warp_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint8_t s_perm[WARPS][kMaxSegments];
-    __shared__ int s_item;
-    __shared__ volatile int s_hit;
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long queued = (long long)(*P.q_head >> 32);
     const int total = (int)min(queued, (long long)P.q_cap);
     uint16_t* pairs = reinterpret_cast<uint16_t*>(smem) + (size_t)warp * P.pairs_per_warp;
+    const GroupLanes GL = group_lanes<M>();
+    for (;;) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(P.finish_counter, 1);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= total) break;
+        const int ro = P.q_rows[i];
+        if (ro < 0) continue;  // the probe walked this pair on
+        const int2 pe = P.q_pairs[i];
+        const float4 h0 = P.env_hdr[2 * pe.y + 0];
+        const float4 h1 = P.env_hdr[2 * pe.y + 1];
+        const uint32_t shape = __float_as_uint(h1.w);
+        const int np = (int)(shape & 0xffffu);
+        const int W = (int)(shape >> 16);
+        const float4* prim = P.blobs + __float_as_uint(h0.w);
+        const uint64_t* masks = reinterpret_cast<const uint64_t*>(prim + (size_t)np * kPrimF4);
+        check_pair<M, 3>(P, pe.y, pe.x, ro, prim, masks, np, W, pairs, s_perm[warp], GL);
+    }
+}
+
+template <class M, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finish_kernel(CheckParams P) {
+    constexpr int G = M::num_env_groups;
+    constexpr int GB = group_bits<M>();
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint8_t s_perm[WARPS][kMaxSegments];
+    __shared__ int s_item, s_C;
+    __shared__ volatile int s_hit;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long queued = (long long)(*P.q_head >> 32);
+    const int total = (int)min(queued, (long long)P.q_cap);
+    // Warp 0 culls and compacts each pair once into the CTA's list (all the
+    // warps' buffers together); a pair whose list would not fit falls back to
+    // per-warp lists (each warp its own copy, walked in segments).
+    uint16_t* cta_pairs = reinterpret_cast<uint16_t*>(smem);
+    const int cta_cap = WARPS * P.pairs_per_warp;
+    uint16_t* pairs = cta_pairs + (size_t)warp * P.pairs_per_warp;
     const GroupLanes GL = group_lanes<M>();
     for (;;) {
         if (threadIdx.x == 0) {
@@ -982,7 +1240,7 @@ __global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finis
         const int ro = P.q_rows[i];
         const int2 pe = ro >= 0 ? P.q_pairs[i] : make_int2(0, 0);
         if (ro >= 0) {  // ro < 0: the probe walked this pair on
-            const int env = pe.y;
+            const int env = pe.y, e = pe.x;
             const float4 h0 = P.env_hdr[2 * env + 0];
             const float4 h1 = P.env_hdr[2 * env + 1];
             const uint32_t shape = __float_as_uint(h1.w);
@@ -990,7 +1248,61 @@ __global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finis
             const int W = (int)(shape >> 16);
             const float4* prim = P.blobs + __float_as_uint(h0.w);
             const uint64_t* masks = reinterpret_cast<const uint64_t*>(prim + (size_t)np * kPrimF4);
-            check_pair<M, 2>(P, env, pe.x, ro, prim, masks, np, W, pairs, s_perm[warp], GL, warp, WARPS, &s_hit);
+            const int n = P.steps[e];
+            const int nseg = 4 * n;
+            if (warp == 0) {
+                // A queued pair passed the probe's self-collision test and has
+                // candidates; the cull below repeats the probe's exactly.
+                const int code = lane < G ? P.edge_tri[(size_t)e * G + lane] : -1;
+                auto mask_word = [&](int w) {
+                    const int tx = code & 1023, ty = (code >> 10) & 1023, tz = code >> 20;
+                    return __ldg(masks + tx * W + w) & __ldg(masks + (kGridTri + ty) * W + w) &
+                           __ldg(masks + (2 * kGridTri + tz) * W + w);
+                };
+                int cnt = 0;
+                if (code >= 0 && np > 0)
+                    for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
+                int off = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(kFull, off, o);
+                    if (lane >= o) off += y;
+                }
+                const int C = __shfl_sync(kFull, off, 31);
+                off -= cnt;
+                const bool fits = C <= cta_cap && nseg <= kMaxSegments;
+                if (fits && cnt > 0) {
+                    int idx = off;
+                    for (int w = 0; w < W; ++w) {
+                        uint64_t m = mask_word(w);
+                        while (m) {
+                            const int b = __ffsll((long long)m) - 1;
+                            cta_pairs[idx++] = (uint16_t)(((w * 64 + b) << GB) | lane);
+                            m &= m - 1;
+                        }
+                    }
+                }
+                if (fits) learned_perm(P, ro, nseg, s_perm[0]);
+                if (lane == 0) {
+                    s_C = fits ? C : -1;
+                    if (fits && P.counters) atomicAdd(P.counters + 1, (unsigned long long)C);
+                }
+            }
+            __syncthreads();
+            const int C = s_C;
+            if (C > 0) {
+                bool undecided = false;
+                WalkStats st;
+                walk_pairs<M, 2>(P.table, (size_t)P.offs[e], n, C, cta_pairs, prim, np, s_perm[0], 0, GL, undecided,
+                                 st, [] { return false; }, 32 * warp, -1, WARPS, &s_hit);
+                if (lane == 0 && P.counters) {
+                    atomicAdd(P.counters + 2, st.chunks);
+                    atomicAdd(P.counters + 3, st.gates);
+                    atomicAdd(P.counters + 4, st.leaf);
+                }
+            } else if (C < 0) {
+                check_pair<M, 2>(P, env, e, ro, prim, masks, np, W, pairs, s_perm[warp], GL, warp, WARPS, &s_hit);
+            }
         }
         __syncthreads();  // every warp is done with this pair (and with s_item)
         if (threadIdx.x == 0 && ro >= 0) {
@@ -1029,7 +1341,8 @@ __device__ __forceinline__ void write_features(const float* q, const float* code
 }
 
 // Features of every queued pair's segments: row ro + j is segment j scored at
-// its middle sample k = 8 j + 4.  Eight lanes per queue entry (four entries per
+// its last sample k = 8 j + 7, the first one the finish walk checks.  Eight
+// lanes per queue entry (four entries per
 // warp in flight, grid-strided), each lane one segment at a time: the loads
 // of an entry form a dependent chain, so several entries per warp hide it.
 constexpr int kFeatureLanes = 8;
@@ -1055,10 +1368,60 @@ __global__ void queue_features_kernel(CheckParams P, const float* __restrict__ e
             t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
         }
         for (int seg = sl; seg < 4 * n; seg += kFeatureLanes) {
-            edge_sample<M::dof>(s, t, n, seg * kSegment + kSegment / 2, q);
+            edge_sample<M::dof>(s, t, n, seg * kSegment + kSegment - 1, q);
             write_features<M>(q, code + (size_t)env * kEnvCode, x + (size_t)(ro + seg) * kMlpIn);
         }
     }
+}
+
+// Inline learned order, features: row c * S + s (S = the check's segments,
+// offs[E] / 8) is segment s of its edge scored at its last sample with the
+// code of environment cluster c.  One thread per row.
+template <class M>
+__global__ void cluster_features_kernel(CheckParams P, const float* __restrict__ edges,
+                                        const float* __restrict__ centroids, int K, const int* __restrict__ row_edge,
+                                        uint16_t* __restrict__ x) {
+    const long long S = P.total_segs;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S * K) return;
+    const int c = (int)(i / S);
+    const int sg = (int)(i - (long long)c * S);
+    const int e = row_edge[(size_t)sg * kSegment];  // segments never straddle edges (offs[e] % 32 == 0)
+    const int j = sg - P.offs[e] / kSegment;
+    float s[M::dof], t[M::dof], q[M::dof];
+#pragma unroll
+    for (int d = 0; d < M::dof; ++d) {
+        s[d] = edges[(size_t)e * 2 * M::dof + d];
+        t[d] = edges[(size_t)e * 2 * M::dof + M::dof + d];
+    }
+    edge_sample<M::dof>(s, t, P.steps[e], j * kSegment + kSegment - 1, q);
+    write_features<M>(q, centroids + (size_t)c * kEnvCode, x + (size_t)i * kMlpIn);
+}
+
+// Inline learned order, permutations: one warp per (cluster c, edge e).
+// Lane block t is scored by the segment holding its last sample t n + n - 1
+// (row c * S + offs[e] / 8 + segment); blocks are ranked by descending score,
+// ties (blocks of one segment) by descending index, so a segment is walked
+// from its end back, and block 0 is ranked first.  perms[(c * E + e) * 32 +
+// rank] = block.
+template <class M>
+__global__ void cluster_perm_kernel(CheckParams P, int K, uint8_t* __restrict__ perms) {
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int E = P.num_edges;
+    if (warp >= (long long)K * E) return;
+    const int c = (int)(warp / E);
+    const int e = (int)(warp - (long long)c * E);
+    const int n = P.steps[e];
+    float v = P.logits[(size_t)c * P.total_segs + P.offs[e] / kSegment + (lane * n + n - 1) / kSegment];
+    v = isnan(v) ? -INFINITY : v;
+    if (lane == 0) v = INFINITY;
+    int rank = 0;
+    for (int u = 0; u < kLanes; ++u) {
+        const float vu = __shfl_sync(kFull, v, u);
+        rank += (vu > v || (vu == v && u > lane)) ? 1 : 0;
+    }
+    perms[((size_t)c * E + e) * kLanes + rank] = (uint8_t)lane;
 }
 
 // Training rows: row i draws (environment, edge, sample) from a hash of
@@ -1072,11 +1435,63 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
     return z ^ (z >> 31);
 }
 
+// Environment verdict of one sample-table row against environment env, one
+// thread: each link group's bound against every primitive and, once some
+// primitive hits it, the group's leaves against every primitive -- the
+// reference's gate semantics (fkcc, src/utils.cuh:806-1190).  Self-collision
+// is not part of it (env-independent, decided per edge before any walk).
+template <class M>
+__device__ __forceinline__ bool sample_hits_env(const CheckParams& P, int env, size_t row) {
+    constexpr int G = M::num_env_groups;
+    const float4 hd0 = P.env_hdr[2 * env], hd1 = P.env_hdr[2 * env + 1];
+    const float4* rec = P.blobs + __float_as_uint(hd0.w);
+    const int np = (int)(__float_as_uint(hd1.w) & 0xffffu);
+    const float4* r = P.table + table_index<M>(row, 0);  // sphere s at r[s * M::table_tile]
+    const DevTables<M>& T = tab<M>();
+    for (int g = 0; g < G; ++g) {
+        float4 b = r[g * M::table_tile];
+        b.w += kEnvInflate;
+        bool gate = false;
+        for (int p = 0; p < np && !gate; ++p) gate = sphere_hits_prim(b, rec + p * kPrimF4);
+        if (!gate) continue;
+        for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1]; ++li) {
+            float4 l = r[(G + li) * M::table_tile];
+            l.w += kEnvInflate;
+            for (int p = 0; p < np; ++p)
+                if (sphere_hits_prim(l, rec + p * kPrimF4)) return true;
+        }
+    }
+    return false;
+}
+
+// Learned-order population: the environment verdict of every sample of every
+// queued pair (one warp per queue entry, lanes over the 32 n samples):
+// lab[8 ro + k] for sample k of the entry whose first MLP row is ro, and
+// y[ro + j] = the verdict at segment j's scored sample 8 j + 7.
+template <class M>
+__global__ void queue_labels_kernel(CheckParams P, uint8_t* __restrict__ lab, uint8_t* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const long long queued = (long long)(*P.q_head >> 32);
+    const int total = (int)min(queued, (long long)P.q_cap);
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const int ro = P.q_rows[i];
+        if (ro < 0) continue;
+        const int2 pe = P.q_pairs[i];
+        const int n = P.steps[pe.x];
+        const size_t row0 = (size_t)P.offs[pe.x];
+        for (int k = lane; k < kLanes * n; k += 32) {
+            const uint8_t h = sample_hits_env<M>(P, pe.y, row0 + (size_t)k) ? 1 : 0;
+            lab[(size_t)ro * kSegment + k] = h;
+            if ((k & (kSegment - 1)) == kSegment - 1) y[ro + k / kSegment] = h;
+        }
+    }
+}
+
 template <class M>
 __global__ void training_rows_kernel(CheckParams P, const float* __restrict__ edges, const float* __restrict__ code,
                                      long long rows, unsigned long long seed, uint16_t* __restrict__ x,
                                      uint8_t* __restrict__ y) {
-    constexpr int G = M::num_env_groups;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const unsigned long long h1 = mix64(seed ^ (unsigned long long)i), h2 = mix64(h1), h3 = mix64(h2);
@@ -1092,25 +1507,7 @@ __global__ void training_rows_kernel(CheckParams P, const float* __restrict__ ed
     }
     edge_sample<M::dof>(s, t, n, k, q);
     write_features<M>(q, code + (size_t)env * kEnvCode, x + (size_t)i * kMlpIn);
-    const float4 hd0 = P.env_hdr[2 * env], hd1 = P.env_hdr[2 * env + 1];
-    const float4* rec = P.blobs + __float_as_uint(hd0.w);
-    const int np = (int)(__float_as_uint(hd1.w) & 0xffffu);
-    const float4* row = P.table + table_index<M>((size_t)P.offs[e] + k, 0);  // stride M::table_tile
-    const DevTables<M>& T = tab<M>();
-    bool hit = false;
-    for (int g = 0; g < G && !hit; ++g) {
-        float4 b = row[g * M::table_tile];
-        b.w += kEnvInflate;
-        bool gate = false;
-        for (int p = 0; p < np && !gate; ++p) gate = sphere_hits_prim(b, rec + p * kPrimF4);
-        if (!gate) continue;
-        for (int li = T.leaf_begin[g]; li < T.leaf_begin[g + 1] && !hit; ++li) {
-            float4 l = row[(G + li) * M::table_tile];
-            l.w += kEnvInflate;
-            for (int p = 0; p < np && !hit; ++p) hit = sphere_hits_prim(l, rec + p * kPrimF4);
-        }
-    }
-    y[i] = hit ? 1 : 0;
+    y[i] = sample_hits_env<M>(P, env, (size_t)P.offs[e] + k) ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ records variant
@@ -1253,16 +1650,17 @@ template <class M, int W>
 cudaError_t launch_finish_w(CheckParams P, cudaStream_t st) {
     P.pairs_per_warp = std::min((P.max_prims * M::num_env_groups + 7) & ~7, kPairCap);
     const size_t smem = (size_t)W * P.pairs_per_warp * sizeof(uint16_t);
-    cudaError_t err = cudaFuncSetAttribute(finish_kernel<M, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = P.finish_split ? finish_kernel<M, W> : finish_warp_kernel<M, W>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finish_kernel<M, W>, W * 32, smem);
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
     if (err != cudaSuccess) return err;
     err = cudaMemsetAsync(P.finish_counter, 0, sizeof(int), st);
     if (err != cudaSuccess) return err;
-    finish_kernel<M, W><<<std::max(per_sm, 1) * std::max(sms, 1), W * 32, smem, st>>>(P);
+    kern<<<std::max(per_sm, 1) * std::max(sms, 1), W * 32, smem, st>>>(P);
     return cudaGetLastError();
 }
 
@@ -1271,6 +1669,7 @@ cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st, int mode) {
     switch (mode) {
         case 1: return launch_check_wm<M, W, 1>(P, E, st);
         case 2: return launch_finish_w<M, W>(P, st);
+        case 4: return launch_check_wm<M, W, 4>(P, E, st);
         default: return launch_check_wm<M, W, 0>(P, E, st);
     }
 }
@@ -1348,11 +1747,36 @@ cudaError_t run_queue_features(const PipelineArgs& a, const float* env_code, uin
 }
 
 template <class M>
+cudaError_t run_cluster_order_inputs(const PipelineArgs& a, const float* centroids, int K, uint16_t* x,
+                                     cudaStream_t st) {
+    const long long rows = (long long)K * a.total_segs;
+    if (rows <= 0) return cudaSuccess;
+    cluster_features_kernel<M><<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(params_of(a), a.d_edges, centroids, K,
+                                                                               a.row_edge, x);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t run_cluster_perms(const PipelineArgs& a, int K, uint8_t* perms, cudaStream_t st) {
+    const long long warps = (long long)K * a.num_edges;
+    if (warps <= 0) return cudaSuccess;
+    cluster_perm_kernel<M><<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(params_of(a), K, perms);
+    return cudaGetLastError();
+}
+
+template <class M>
 cudaError_t run_training_rows(const PipelineArgs& a, const float* env_code, long long rows, unsigned long long seed,
                               uint16_t* x, uint8_t* y, cudaStream_t st) {
     if (rows <= 0) return cudaSuccess;
     training_rows_kernel<M><<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(params_of(a), a.d_edges, env_code, rows,
                                                                            seed, x, y);
+    return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t run_queue_labels(const PipelineArgs& a, uint8_t* lab, uint8_t* y, int grid, cudaStream_t st) {
+    if (grid <= 0) return cudaSuccess;
+    queue_labels_kernel<M><<<grid, 256, 0, st>>>(params_of(a), lab, y);
     return cudaGetLastError();
 }
 
@@ -1386,6 +1810,9 @@ RobotOps robot_ops_of(int robot, cudaError_t (*upload)()) {
     o.check_mode = run_check_mode<M>;
     o.queue_features = run_queue_features<M>;
     o.training_rows = run_training_rows<M>;
+    o.queue_labels = run_queue_labels<M>;
+    o.cluster_features = run_cluster_order_inputs<M>;
+    o.cluster_perms = run_cluster_perms<M>;
     o.check_records = run_check_records<M>;
     return o;
 }

@@ -33,15 +33,23 @@ UNIT = "edges/s"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
-def committed_traffic(workload_name_):
-    """DRAM bytes of one check_kernel launch on a full-size workload, from the
-    committed ncu summary (None when the workload has no capture)."""
+COUNTS_FILE = os.path.join("profiles", "check_kernel_counts.md")
+
+
+def committed_counts(workload_name_):
+    """Per-pair counts of the plain-order check kernel on a workload, from the
+    committed ncu summary: warp instructions executed, FP32 FFMA / FADD / FMUL
+    thread instructions and DRAM bytes, each divided by the pairs of the
+    captured launch (None when the workload has no capture)."""
     import re
-    path = os.path.join(ROOT, "profiles", "check_kernel_dram_traffic.md")
+    path = os.path.join(ROOT, COUNTS_FILE)
     if not os.path.exists(path):
         return None
-    m = re.search(r"^traffic_bytes %s (\d+)$" % re.escape(workload_name_), open(path).read(), re.M)
-    return int(m.group(1)) if m else None
+    m = re.search(r"^counts %s (.*)$" % re.escape(workload_name_), open(path).read(), re.M)
+    if not m:
+        return None
+    f = m.group(1).split()
+    return {f[i]: float(f[i + 1]) for i in range(0, len(f) - 1, 2)}
 
 
 def metric_of(name, N):
@@ -120,6 +128,7 @@ def parse():
     p.add_argument("--no-parity", action="store_true", help="skip the full-size parity leg against the reference "
                                                              "CUDA kernel")
     p.add_argument("--flop-sample", type=int, default=20000)
+    p.add_argument("--no-others", action="store_true", help="skip the Fetch, Baxter and stress workloads")
     p.add_argument("--profile-order", default=None, choices=["plain", "learned"],
                    help="profiling run: only `--warmup` + `--steps` eager checks in this order (launch config "
                         "--profile-launch, MLP at its seeded initialisation), no training, tuning or baselines")
@@ -309,23 +318,45 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+TRAIN_QUEUE_MIN_ITEMS = 128  # the lowest queue threshold the tuner tries: its population holds every higher one's
+
+
 def train_proposal(chk, args):
-    """Train the collision-likelihood MLP (untimed) on checker labels of
-    uneven-style environments and edges with seeds disjoint from the benchmark's."""
+    """Train the collision-likelihood MLP (untimed) on the population the
+    learned order acts on -- the segments of the pairs its probe queues --
+    with checker labels, over environments and edges with seeds disjoint from
+    the benchmark's."""
     from bcc import mlp, workload
     t0 = time.perf_counter()
     chk.upload(workload.gen_envs(args.workload, args.train_envs, seed=1000))
     chk.mlp_set_params(mlp.init_params(1000))
-    losses, pos = chk.mlp_train(workload.gen_edges(args.workload, args.edges, seed=1000),
-                                num_samples=args.train_samples, epochs=args.train_epochs, batch=16384, lr=2e-3,
-                                seed=1000, robot=workload.robot_of(args.workload))
-    return {"train_samples": args.train_samples, "epochs": args.train_epochs, "epoch_loss": [float(v) for v in losses],
+    losses, pos, rows = chk.mlp_train_queued(workload.gen_edges(args.workload, args.edges, seed=1000),
+                                             num_samples=args.train_samples, queue_min_items=TRAIN_QUEUE_MIN_ITEMS,
+                                             epochs=args.train_epochs, batch=16384, lr=2e-3, seed=1000,
+                                             robot=workload.robot_of(args.workload))
+    return {"train_rows": rows, "epochs": args.train_epochs, "epoch_loss": [float(v) for v in losses],
             "train_positive_fraction": pos, "train_seconds": time.perf_counter() - t0,
-            "data": "checker-labelled samples of %s environments/edges with seed 1000 (benchmark uses seed 0)" % (
-                args.workload)}
+            "data": "segments (scored at their last sample) of the pairs the probe queues at threshold %d, "
+                    "checker-labelled, %d %s environments x %d edges with seed 1000 (benchmark uses seed 0)" % (
+                        TRAIN_QUEUE_MIN_ITEMS, args.train_envs, args.workload, args.edges or 0)}
 
 
-def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev, robot="panda"):
+def proposal_ranking(chk, edges, queue_min_items, robot):
+    """Ranking quality on the benchmark's own queued population (held out:
+    trained on other seeds), for the trained network and for the same network
+    untrained (its seeded initialisation): AUC of the segment scores and the
+    sample ranks walked to the first hit in the plain, learned and perfect
+    orders (bcc_mlp_rank_metrics)."""
+    from bcc import mlp
+    trained = chk.mlp_get_params()
+    out = {"queue_min_items": queue_min_items, "trained": chk.mlp_rank_metrics(edges, queue_min_items, robot=robot)}
+    chk.mlp_set_params(mlp.init_params(1000))
+    out["untrained"] = chk.mlp_rank_metrics(edges, queue_min_items, robot=robot)
+    chk.mlp_set_params(trained)
+    return out
+
+
+def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev, robot="panda", eager_reps=3):
     """Timed region: `steps` graph-captured (persistent-kernel) checks, L2 flushed
     between steps outside the timed events; then an untimed eager pass for the
     per-stage breakdown."""
@@ -347,7 +378,7 @@ def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev,
     torch.cuda.synchronize()
     total_ms = sum(x.elapsed_time(y) for x, y in evs)
     stage_tot, check_ms = {}, []
-    reps = 3
+    reps = eager_reps
     for i in range(reps):
         flush.fill_(float(i))
         step(False)
@@ -356,7 +387,65 @@ def time_order(chk, d_edges, d_res, E, order, stream, steps, warmup, flush, dev,
         check_ms.append(st["check"])
         for k, v in st.items():
             stage_tot[k] = stage_tot.get(k, 0.0) + v
-    return total_ms, check_ms, {k: v / reps for k, v in stage_tot.items()}
+    return total_ms, check_ms, {k: v / max(reps, 1) for k, v in stage_tot.items()}
+
+
+OTHER_WORKLOADS = ("multi_fetch", "multi_baxter", "stress")
+# Parity subsample of the other workloads against the reference CUDA kernel:
+# the first envs x first edges of the full inputs (all of them for Fetch and
+# Baxter; 1000 x 10000 of the stress run's 10000 x 100000).
+PARITY_SUBSAMPLE = {"multi_fetch": (500, 5000), "multi_baxter": (500, 5000), "stress": (1000, 10000)}
+
+
+def measure_workload(chk, name, steps, warmup, flush, dev, parity, train_envs=2000, train_edges=5000):
+    """One further workload at full size, compactly: the network trained on
+    that workload's own queued population (seed 1000), launch configuration
+    autotuned per order, both orders timed (graph replays, L2 flushed, CUDA
+    events), verdicts of the orders compared, and parity against the
+    reference CUDA kernel on a stated subsample (mismatches adjudicated)."""
+    import torch
+    from bcc import mlp, workload
+    robot = workload.robot_of(name)
+    stream = torch.cuda.current_stream()
+    chk.upload(workload.gen_envs(name, train_envs, seed=1000))
+    chk.mlp_set_params(mlp.init_params(1000))
+    _, _, rows = chk.mlp_train_queued(workload.gen_edges(name, train_edges, seed=1000), num_samples=10_000_000,
+                                      queue_min_items=TRAIN_QUEUE_MIN_ITEMS, epochs=2, batch=16384, lr=2e-3,
+                                      seed=1000, robot=robot)
+    envs = workload.gen_envs(name, seed=0)
+    edges = workload.gen_edges(name, seed=0)
+    N, E = envs.num_envs, len(edges)
+    chk.upload(envs)
+    d_edges = torch.from_numpy(edges).to(f"cuda:{dev}")
+    d_res = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
+    d_res2 = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
+    n_tune = min(E, 10000, max(1000, 20_000_000 // max(N, 1)))
+    tuned = {o: chk.autotune(edges[:n_tune], order=o, robot=robot) for o in ("plain", "learned")}
+    ms = {}
+    for order, res in (("plain", d_res), ("learned", d_res2)):
+        chk.set_launch_config(**tuned[order])
+        total_ms, _, _ = time_order(chk, d_edges, res, E, order, stream, steps, warmup, flush, dev, robot,
+                                    eager_reps=0)
+        ms[order] = total_ms / steps
+    learned_pairs = chk.last_learned_pairs()
+    mismatch = int((d_res != d_res2).sum().item())
+    out = {"workload": workload_name(name, N, E), "metric": metric_of(name, N), "unit": UNIT, "steps": steps,
+           "warmup": warmup,
+           "orders": {o: {"value": N * E / (ms[o] * 1e-3), "ms_per_step": ms[o], "launch": tuned[o]} for o in ms},
+           "learned_over_plain": ms["plain"] / ms["learned"], "verdict_mismatches_learned_vs_plain": mismatch,
+           "queued_pairs_per_step": learned_pairs, "train_rows": rows}
+    if parity:
+        nv, ne = PARITY_SUBSAMPLE[name]
+        sub_envs = envs.subset(np.arange(min(nv, N)))
+        verdicts = {"plain": d_res[:ne, :nv].cpu().numpy(), "learned": d_res2[:ne, :nv].cpu().numpy()}
+        par, ref_cuda = parity_vs_reference(sub_envs, edges[:ne], verdicts, robot, iters=1)
+        if par is not None:
+            par["subsample"] = "first %d envs x first %d edges" % (sub_envs.num_envs, min(ne, E))
+            out["parity"] = par
+            out["reference_cuda"] = ref_cuda
+    del d_res, d_res2, d_edges
+    torch.cuda.empty_cache()
+    return out
 
 
 def mlp_roofline(chk, dev, rows=1 << 22, reps=5):
@@ -398,6 +487,8 @@ def run_profile(args, local):
     chk.set_launch_config(edges_per_cta=tile, warps=warps, persistent=persistent)
     if len(launch) > 3:
         chk.set_launch_config(queue_min_items=launch[3])
+    if len(launch) > 4:
+        chk.set_launch_config(finish_split=launch[4])
     for _ in range(args.warmup + args.steps):
         chk.check(edges, order=args.profile_order, robot=robot)
     torch.cuda.synchronize()
@@ -421,7 +512,6 @@ def run_ours(args, world, rank, local, dist):
     edges = rank_edges(args.workload, args.edges, rank)
     N, E = envs.num_envs, len(edges)
     chk.upload(envs)
-    proposal.update(chk.mlp_evaluate(edges, 1 << 20, seed=7, robot=robot))
     chk.set_profiling(True)
     stream = torch.cuda.current_stream()
     d_edges = torch.from_numpy(edges).to(f"cuda:{dev}")
@@ -471,6 +561,10 @@ def run_ours(args, world, rank, local, dist):
     torch.cuda.synchronize()
     learned_rows = chk.last_learned_rows()
     learned_pairs = chk.last_learned_pairs()
+    ranking = proposal_ranking(chk, edges, tuned["learned"]["queue_min_items"], robot)
+    proposal["uniform_samples"] = dict(chk.mlp_evaluate(edges, 1 << 20, seed=7, robot=robot),
+                                       note="misprediction against the exact checker on 2^20 uniformly drawn "
+                                            "(env, edge, sample) triples of the benchmark inputs")
 
     # e2e: the public host API (pinned host edges in, verdicts out), per step.
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
@@ -500,31 +594,57 @@ def run_ours(args, world, rank, local, dist):
             "learned_over_plain": ms["plain"] / ms["learned"],
             "verdict_mismatches_learned_vs_plain": mismatch,
             "proposal": dict(proposal, scored_segments_per_step=learned_rows, queued_pairs_per_step=learned_pairs,
-                             queued_fraction=learned_pairs / float(N * E)),
+                             queued_fraction=learned_pairs / float(N * E), ranking=ranking),
             "gpu_launches": (6 + 9) * args.steps,  # plain: 6 launches per step; learned: 9
             "clocks": clk.summary()}
     line["e2e"] = {"value": world * N * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(edges.nbytes),
                    "d2h_bytes_per_step": int(N * E),
                    "path": "bcc_check (host edges in, host verdicts out; bcc_opts.use_graph = 1)"}
-    # Roofline of the dominant kernel (environment check, plain order):
-    # algorithmic FLOPs of the reference plain order per launch / mean
-    # CUDA-event duration of the launch.
-    peak = measure_fp32_peak(dev)
-    flops, rel_err = algorithmic_flops(envs, edges, args.flop_sample, robot)
+    # Roofline of the dominant kernel (environment check, plain order).  It is
+    # bound by instruction issue (integer/logic and FP32 SIMT work on L2- and
+    # shared-memory-resident inputs, DRAM a few per cent busy), so the roofline
+    # is issue slots: achieved = warp instructions per launch (the committed ncu
+    # count per pair x this launch's pairs) / the launch's CUDA-event duration,
+    # peak = 148 SMs x 4 issue slots per cycle x the SM clock sampled during the
+    # timed region.  The executed FP32 arithmetic is reported beside it against
+    # the FMA probe's peak, and the reference's plain-order work (oracle count)
+    # as the work the design avoids.
     chk_ms = statistics.mean(results["plain"][1])
-    achieved = flops / (chk_ms * 1e-3) / 1e12
-    traffic = committed_traffic(args.workload) if (args.envs is None and args.edges is None) else None
-    line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "traffic": traffic,
-                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one check_kernel "
-                                          "launch on this workload (profiles/check_kernel_dram_traffic.md)"
-                        if traffic else None,
-                        "kernel": "check_kernel (plain order)", "kernel_ms": chk_ms,
-                        "algorithmic_flops_per_launch": flops, "flop_estimate_rel_stderr": rel_err,
-                        "peak_source": "FP32 FMA probe kernel measured in this run (bcc_measure_fp32_peak); "
-                                       "MEASURED_PEAKS.json has no FP32 figure",
-                        "note": "algorithmic FLOPs = the reference's plain-order work (oracle count); "
-                                "work this kernel skips (hoisted FK/self checks, culling) raises frac"}
+    counts = committed_counts(args.workload) if (args.envs is None and args.edges is None) else None
+    clocks = line["clocks"]
+    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    import torch as _t
+    sms = _t.cuda.get_device_properties(dev).multi_processor_count
+    issue_peak = sms * 4 * sm_mhz * 1e6 / 1e9  # G warp-instructions / s
+    fp32_peak = measure_fp32_peak(dev)
+    ref_flops, rel_err = algorithmic_flops(envs, edges, args.flop_sample, robot)
+    pairs = float(N * E)
+    roof = {"bound": "issue", "unit": "G warp-instructions/s", "peak": issue_peak,
+            "peak_source": "%d SMs x 4 warp-instruction issue slots per cycle x %.0f MHz (median SM clock sampled "
+                           "during the timed region)" % (sms, sm_mhz),
+            "kernel": "check_kernel (plain order)", "kernel_ms": chk_ms,
+            "work_avoided": {"reference_plain_order_flops_per_launch": ref_flops,
+                             "flop_estimate_rel_stderr": rel_err,
+                             "note": "FP32 FLOPs the reference's literal plain order spends on these pairs (oracle "
+                                     "count); hoisted FK and self checks, culling and the finer early exit avoid "
+                                     "most of it"}}
+    if counts:
+        inst = counts["inst_per_pair"] * pairs
+        flop = (2.0 * counts["ffma_per_pair"] + counts["fadd_per_pair"] + counts["fmul_per_pair"]) * pairs
+        roof.update({"achieved": inst / (chk_ms * 1e-3) / 1e9, "frac": inst / (chk_ms * 1e-3) / 1e9 / issue_peak,
+                     "traffic": counts["dram_bytes_per_pair"] * pairs,
+                     "executed_warp_instructions_per_launch": inst,
+                     "counts_source": "ncu sm__inst_executed.sum, smsp__sass_thread_inst_executed_op_{ffma,fadd,"
+                                      "fmul}_pred_on.sum, dram__bytes_{read,write}.sum of one plain check_kernel "
+                                      "launch, per pair, scaled by this launch's pairs (%s)" % COUNTS_FILE,
+                     "fp32": {"achieved_tflops": flop / (chk_ms * 1e-3) / 1e12, "peak": fp32_peak,
+                              "frac": flop / (chk_ms * 1e-3) / 1e12 / fp32_peak,
+                              "peak_source": "FP32 FMA probe kernel measured in this run (bcc_measure_fp32_peak)"}})
+        roof["work_avoided"]["factor"] = ref_flops / flop
+    else:
+        roof.update({"achieved": None, "frac": None, "traffic": None,
+                     "note": "no committed ncu counts for this workload / size"})
+    line["roofline"] = roof
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     bf16_peak = peaks.get("bf16_tflops")
@@ -541,6 +661,13 @@ def run_ours(args, world, rank, local, dist):
             line["reference_cuda"] = ref_cuda
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(envs, edges, robot)
+    if world == 1 and args.workload == WORKLOAD and args.envs is None and args.edges is None and not args.no_others:
+        others = {}
+        with ClockSampler(dev) as clk2:
+            for name in OTHER_WORKLOADS:
+                others[name] = measure_workload(chk, name, steps=3, warmup=2, flush=flush, dev=dev,
+                                                parity=not args.no_parity)
+        line["other_workloads"] = dict(others, clocks=clk2.summary())
     chk.close()
     print(json.dumps(line))
 

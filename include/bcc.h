@@ -211,6 +211,39 @@ bcc_status bcc_mlp_gradients(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t* 
 bcc_status bcc_mlp_train(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
                          int64_t num_samples, int32_t epochs, int32_t batch, float lr, uint64_t seed,
                          float* h_epoch_loss, float* h_positive_fraction);
+/*
+ * Train on the population the learned order acts on: the (environment, edge)
+ * pairs that the probe -- the plain walk of each pair's rank 0, its first
+ * sample -- leaves undecided with at least queue_min_items (sample, pair)
+ * items to go, over the uploaded environments and the given host edges.  One
+ * row per segment of such a pair (features at the segment's scored sample, its
+ * last one), labelled by this library's exact check of that sample; a seeded
+ * shuffle of at most num_samples of them, Adam, `epochs` passes in batches of
+ * `batch` rows.  h_rows (may be NULL) receives the rows used; fewer than one
+ * batch returns BCC_ERR_INVALID_ARGUMENT.
+ */
+bcc_status bcc_mlp_train_queued(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges,
+                                int32_t resolution, int32_t queue_min_items, int64_t num_samples, int32_t epochs,
+                                int32_t batch, float lr, uint64_t seed, float* h_epoch_loss,
+                                float* h_positive_fraction, int64_t* h_rows);
+/*
+ * Ranking quality of the current network on the learned order's population
+ * (the pairs queued at queue_min_items, as for bcc_mlp_train_queued), judged
+ * by this library's exact per-sample checks.  h_metrics[0..12]:
+ *   [0] queued pairs, [1] scored segments, [2] colliding fraction of the queued
+ *   pairs, [3] colliding fraction of the scored samples, [4] AUC of the segment
+ *   scores against the scored samples' verdicts; sample ranks walked after the
+ *   probe until the first hit, mean over the colliding queued pairs, in the
+ *   [5] plain order (reference ranks 1, 2, ...), [6] learned order (segments by
+ *   descending score, each from its last sample), [7] perfect order (1);
+ *   [8..10] the same means over all queued pairs (collision-free pairs walk
+ *   all their samples); [11] share of the perfect order's saving over the plain
+ *   order that the learned order realises on the colliding pairs; [12]
+ *   misprediction rate of the scored samples (sign of the logit vs verdict).
+ */
+bcc_status bcc_mlp_rank_metrics(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges,
+                                int32_t resolution, int32_t queue_min_items, double* h_metrics,
+                                int32_t max_metrics);
 /* Held-out metrics on fresh samples: [0] mean BCE, [1] misprediction rate (sign
  * of the logit vs the checker's verdict), [2] false-positive rate, [3]
  * false-negative rate, [4] positive fraction. */
@@ -238,21 +271,32 @@ bcc_status bcc_mlp_train_step(bcc_ctx* ctx, const void* d_x_bf16, const uint8_t*
 bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
 
 /*
- * Launch configuration of the environment check: cfg[0] edges per CTA, cfg[1]
- * warps per CTA (1, 2, 4, 8; lowered automatically when an environment's
- * shared-memory footprint needs it), cfg[2] 1 = persistent kernel pulling
- * (environment, edge tile) work items from an atomic queue, 0 = one CTA per
- * item, cfg[3] learned order: a pair is scored by the MLP only when at least
- * this many (sample, pair) items remain once its rank 0 (first sample) is walked.
+ * Launch configuration of the environment check, BCC_LAUNCH_CONFIG_LEN values:
+ * cfg[0] edges per CTA, cfg[1] warps per CTA (1, 2, 4, 8; lowered
+ * automatically when an environment's shared-memory footprint needs it),
+ * cfg[2] 1 = persistent kernel pulling (environment, edge tile) work items
+ * from an atomic queue, 0 = one CTA per item, cfg[3] learned order: a pair is
+ * scored by the MLP only when at least this many (sample, pair) items remain
+ * once its rank 0 (first sample) is walked, cfg[4] learned order: 1 = each
+ * queued pair's walk split over a CTA's warps, 0 = one warp per queued pair,
+ * cfg[5] learned order: 0 = inline (every pair walks its first sample, then
+ * its other samples in the order the MLP scored for its environment's
+ * cluster, in one pass), 1 = queued (pairs left undecided by a plain probe of
+ * their first sample are scored per pair and finished in a second pass),
+ * cfg[6] inline order: environment clusters, 1..64 (k-means over the
+ * environment codes; the MLP scores each edge's segments once per cluster).
  */
+#define BCC_LAUNCH_CONFIG_LEN 7
 bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg);
 bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg);
 /*
  * Autotuner: times candidate configurations (edges per CTA 32..256, 4 or 8
- * warps, persistent or not; for the learned order jointly with the queue
- * threshold 128..4096 items) on the given host edges against the uploaded
- * environments, timing graph replays, and keeps the fastest
- * in the context; chosen[4] receives it (may be NULL).  order: bcc_order.
+ * warps, persistent or not; for the learned order also the inline order's
+ * cluster count and the queued order's threshold 64..4096 items and finish
+ * mode) on the given host edges against the
+ * uploaded environments, timing graph replays, and keeps the fastest in the
+ * context; chosen[BCC_LAUNCH_CONFIG_LEN] receives it (may be NULL).
+ * order: bcc_order.
  */
 bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t num_edges, int32_t resolution,
                         int32_t order, int32_t* chosen);

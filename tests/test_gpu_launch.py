@@ -61,7 +61,9 @@ def test_autotune_picks_a_valid_config(checker, case):
     assert cfg["edges_per_cta"] in (32, 64, 128, 256) and cfg["warps"] in (4, 8)
     assert np.array_equal(checker.check(edges), base)
     cfg = checker.autotune(edges, order="learned")
-    # the learned order's shape and queue threshold are swept jointly
+    # the learned order's shape, mode, clusters and queue threshold are swept
     assert cfg["edges_per_cta"] in (32, 64, 128, 256) and cfg["warps"] in (4, 8)
-    assert cfg["queue_min_items"] in (128, 256, 512, 1024, 2048, 4096)
+    assert cfg["learned_mode"] in (0, 1) and cfg["clusters"] in (1, 4, 8, 16)
+    if cfg["learned_mode"] == 1:
+        assert cfg["queue_min_items"] in (64, 128, 256, 512, 1024, 2048, 4096)
     assert np.array_equal(checker.check(edges, order="learned"), base)
