@@ -369,9 +369,14 @@ bcc_status prepare_inline(bcc_ctx* ctx, bcc::PipelineArgs& a) {
 // segment) row, tcgen05 MLP scores, per-(cluster, edge) permutations, then one
 // check in which every pair walks rank 0 (sample 0) and then its other samples
 // in its cluster's learned order (mode 4): no queue, no second pass.
+// With one cluster the permutation depends on the edge alone, so the FK
+// kernel writes each edge's table rows in learned order (lane block pi(t) at
+// block position t) and the plain check kernel (mode 0) walks them: the order
+// costs the check kernel nothing.  With several clusters the table stays in
+// sample order and the check kernel (mode 4) maps ranks through each pair's
+// cluster permutation.
 bcc_status run_learned_inline(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::PipelineArgs& a, cudaStream_t st) {
     cudaEvent_t* ev = a.stage_events;
-    BCC_CUDA(ctx, ops->prep(a, st));  // records stage events 1-4
     const int K = ctx->cluster_k;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -380,7 +385,9 @@ bcc_status run_learned_inline(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::Pipel
                                    ctx->mlp.params.as<float>(), ctx->mlp.logits.as<float>(), a.error_flag,
                                    std::max(sms, 1), st));
     BCC_CUDA(ctx, ops->cluster_perms(a, K, ctx->perms.as<uint8_t>(), st));
-    a.mode = 4;
+    a.fk_perm = K == 1 ? ctx->perms.as<uint8_t>() : nullptr;
+    BCC_CUDA(ctx, ops->prep(a, st));  // records stage events 1-4
+    a.mode = K == 1 ? 0 : 4;
     BCC_CUDA(ctx, ops->check_mode(a, st));
     if (ev) cudaEventRecord(ev[5], st);
     return BCC_OK;
@@ -1272,9 +1279,9 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
                 }
     };
     bcc::Tune start = base;
-    if (learned) {  // the inline order at 8 clusters while the shape is swept
+    if (learned) {  // the inline order at one cluster while the shape is swept
         start.learned_mode = 0;
-        start.clusters = 8;
+        start.clusters = 1;
     }
     sweep_shape(start);
     if (learned) {

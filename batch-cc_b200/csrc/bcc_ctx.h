@@ -52,7 +52,7 @@ struct Tune {
     int queue_min_items = 128;
     int finish_split = 0;    // learned order, queued: 1 = split each queued pair over a CTA's warps
     int learned_mode = 0;    // learned order: 0 = inline (per-cluster scores), 1 = queued (per-pair scores)
-    int clusters = 8;        // learned order, inline: environment clusters scored per edge
+    int clusters = 1;        // learned order, inline: environment clusters scored per edge
     bool tuned = false;
 };
 

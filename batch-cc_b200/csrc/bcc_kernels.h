@@ -75,6 +75,7 @@ struct PipelineArgs {
     int total_rows;          // offs[E], read back after the scan
     float4* table;           // [total_rows][num_spheres]
     int* row_edge;           // [total_rows]
+    const uint8_t* fk_perm;  // null, or [E][32] lane-block permutation the FK table is written in
     int* edge_self;          // [E]
     float4* swept;           // [E][groups][2]
     int* edge_tri;           // [E][groups], null = not needed (records check)

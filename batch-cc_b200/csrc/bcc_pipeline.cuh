@@ -145,12 +145,22 @@ __global__ void edge_steps_kernel(const float* __restrict__ edges, int E, int re
 // (env-group bounds, then env leaves, then the rest), one row per (edge,
 // sample) in edge order then sample index order; stored in tiles of
 // M::table_tile rows (table_index).
+// Sample at table position k of edge e: k itself, or with a block
+// permutation (inline learned order, one cluster) lane block perm[e][k / n]'s
+// sample of the same round, so the reference walk over the table visits the
+// samples in learned order.
+__device__ __forceinline__ int table_sample(const uint8_t* __restrict__ perm, int e, int n, int k) {
+    if (!perm) return k;
+    const int blk = k / n;
+    return (int)perm[(size_t)e * kLanes + blk] * n + (k - blk * n);
+}
+
 template <class M>
 __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges, int E,
                                                  const int* __restrict__ steps,
                                                  const int* __restrict__ offs,
                                                  float4* __restrict__ table,
-                                                 int* __restrict__ row_edge) {
+                                                 int* __restrict__ row_edge, const uint8_t* __restrict__ perm) {
     const int total = offs[E];
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= total) return;
@@ -168,7 +178,7 @@ __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges
         s[j] = edges[(size_t)e * 2 * M::dof + j];
         t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
     }
-    edge_sample<M::dof>(s, t, steps[e], k, q);
+    edge_sample<M::dof>(s, t, steps[e], table_sample(perm, e, steps[e], k), q);
     fk_spheres<M>(q, table + table_index<M>(row, 0));
     row_edge[row] = e;
 }
@@ -183,7 +193,7 @@ __global__ void __launch_bounds__(32) fk_staged_kernel(const float* __restrict__
                                                        const int* __restrict__ steps,
                                                        const int* __restrict__ offs,
                                                        float4* __restrict__ table,
-                                                       int* __restrict__ row_edge) {
+                                                       int* __restrict__ row_edge, const uint8_t* __restrict__ perm) {
     static_assert(M::table_tile == 1, "row-major tables only");
     constexpr int NS = M::num_spheres;
     constexpr int STRIDE = NS | 1;
@@ -205,7 +215,7 @@ __global__ void __launch_bounds__(32) fk_staged_kernel(const float* __restrict__
             s[j] = edges[(size_t)e * 2 * M::dof + j];
             t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
         }
-        edge_sample<M::dof>(s, t, steps[e], k, q);
+        edge_sample<M::dof>(s, t, steps[e], table_sample(perm, e, steps[e], k), q);
         fk_spheres<M>(q, srow + threadIdx.x * STRIDE);
         row_edge[row] = e;
     }
@@ -1386,7 +1396,16 @@ __global__ void cluster_features_kernel(CheckParams P, const float* __restrict__
     if (i >= S * K) return;
     const int c = (int)(i / S);
     const int sg = (int)(i - (long long)c * S);
-    const int e = row_edge[(size_t)sg * kSegment];  // segments never straddle edges (offs[e] % 32 == 0)
+    // the segment's edge: segments never straddle edges (offs[e] % 32 == 0);
+    // binary search over the sample offsets (the FK table may not exist yet)
+    const int row = sg * kSegment;
+    int lo = 0, hi = P.num_edges - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.offs[mid] <= row) lo = mid; else hi = mid - 1;
+    }
+    const int e = lo;
+    (void)row_edge;
     const int j = sg - P.offs[e] / kSegment;
     float s[M::dof], t[M::dof], q[M::dof];
 #pragma unroll
@@ -1699,9 +1718,11 @@ cudaError_t run_prep(const PipelineArgs& a, cudaStream_t st) {
             cudaError_t err = cudaFuncSetAttribute(fk_staged_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)smem);
             if (err != cudaSuccess) return err;
-            fk_staged_kernel<M><<<(R + 31) / 32, 32, smem, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
+            fk_staged_kernel<M><<<(R + 31) / 32, 32, smem, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge,
+                                                                  a.fk_perm);
         } else {
-            fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge);
+            fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge,
+                                                           a.fk_perm);
         }
     }
     if (ev) cudaEventRecord(ev[2], st);
