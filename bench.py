@@ -342,14 +342,18 @@ def train_proposal(chk, args):
 
 
 def proposal_ranking(chk, edges, queue_min_items, robot):
-    """Ranking quality on the benchmark's own queued population (held out:
+    """Ranking quality on the benchmark's own pairs that the first-sample probe
+    leaves undecided with at least queue_min_items items to go (held out:
     trained on other seeds), for the trained network and for the same network
-    untrained (its seeded initialisation): AUC of the segment scores and the
-    sample ranks walked to the first hit in the plain, learned and perfect
-    orders (bcc_mlp_rank_metrics)."""
+    untrained (its seeded initialisation), judged by the exact per-sample
+    checks: AUC of the per-pair segment scores and the sample ranks walked to
+    the first hit in the plain, learned and perfect orders
+    (bcc_mlp_rank_metrics)."""
     from bcc import mlp
     trained = chk.mlp_get_params()
-    out = {"queue_min_items": queue_min_items, "trained": chk.mlp_rank_metrics(edges, queue_min_items, robot=robot)}
+    out = {"population": "pairs left undecided by the probe of their first sample, >= %d items to go"
+                         % queue_min_items,
+           "queue_min_items": queue_min_items, "trained": chk.mlp_rank_metrics(edges, queue_min_items, robot=robot)}
     chk.mlp_set_params(mlp.init_params(1000))
     out["untrained"] = chk.mlp_rank_metrics(edges, queue_min_items, robot=robot)
     chk.mlp_set_params(trained)
@@ -556,12 +560,26 @@ def run_ours(args, world, rank, local, dist):
         c = chk.work_counters()
         work[order] = {k: v / max(c["pairs"], 1) for k, v in c.items() if k != "pairs"}
         work[order]["pairs_walked"] = c["pairs"]
+    # What the training adds: the same learned pipeline and launch with the
+    # network at its seeded initialisation (untrained), timed the same way,
+    # and its work counters.
+    from bcc import mlp as _mlp
+    trained_params = chk.mlp_get_params()
+    chk.mlp_set_params(_mlp.init_params(1000))
+    chk.set_launch_config(**tuned["learned"])
+    chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream, robot=robot)
+    torch.cuda.synchronize()
+    c = chk.work_counters()
+    work_untrained = {k: v / max(c["pairs"], 1) for k, v in c.items() if k != "pairs"}
     chk.set_profiling(True)
+    untrained_ms = time_order(chk, d_edges, d_res, E, "learned", stream, args.steps, args.warmup, flush, dev, robot,
+                              eager_reps=0)[0] / args.steps
+    chk.mlp_set_params(trained_params)
     chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream, robot=robot)
     torch.cuda.synchronize()
     learned_rows = chk.last_learned_rows()
     learned_pairs = chk.last_learned_pairs()
-    ranking = proposal_ranking(chk, edges, tuned["learned"]["queue_min_items"], robot)
+    ranking = proposal_ranking(chk, edges, TRAIN_QUEUE_MIN_ITEMS, robot)
     proposal["uniform_samples"] = dict(chk.mlp_evaluate(edges, 1 << 20, seed=7, robot=robot),
                                        note="misprediction against the exact checker on 2^20 uniformly drawn "
                                             "(env, edge, sample) triples of the benchmark inputs")
@@ -592,6 +610,11 @@ def run_ours(args, world, rank, local, dist):
                            "launch": dict(tuned[o], graph=True), "stages_ms_per_step_eager": results[o][2],
                            "work_per_pair": work[o]} for o in results},
             "learned_over_plain": ms["plain"] / ms["learned"],
+            "ablation_untrained_network": {
+                "value": world * N * E / (untrained_ms * 1e-3), "ms_per_step": untrained_ms,
+                "over_plain": ms["plain"] / untrained_ms, "work_per_pair": work_untrained,
+                "note": "the learned pipeline with the same launch, the network at its seeded initialisation "
+                        "(untrained): learned_over_plain minus this over_plain is what the training adds"},
             "verdict_mismatches_learned_vs_plain": mismatch,
             "proposal": dict(proposal, scored_segments_per_step=learned_rows, queued_pairs_per_step=learned_pairs,
                              queued_fraction=learned_pairs / float(N * E), ranking=ranking),
