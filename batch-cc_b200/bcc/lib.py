@@ -273,7 +273,7 @@ class Checker:
         return int(lib().bcc_last_learned_pairs(self._h))
 
     CONFIG = ("edges_per_cta", "warps", "persistent", "queue_min_items", "finish_split", "learned_mode",
-              "clusters")
+              "clusters", "lanes")
 
     def launch_config(self):
         c = (ctypes.c_int32 * len(self.CONFIG))()

@@ -209,6 +209,7 @@ bcc_status prepare(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, i
     a.persistent = ctx->tune.persistent;
     a.queue_min_items = ctx->tune.queue_min_items;
     a.finish_split = ctx->tune.finish_split;
+    a.mode = ctx->tune.lanes == 16 ? 5 : 0;  // the plain walk: whole warp or half-warp per pair
     BCC_CUDA(ctx, ctx->work_counter.ensure(64));
     a.work_counter = ctx->work_counter.as<int>();
     return BCC_OK;
@@ -387,7 +388,7 @@ bcc_status run_learned_inline(bcc_ctx* ctx, const bcc::RobotOps* ops, bcc::Pipel
     BCC_CUDA(ctx, ops->cluster_perms(a, K, ctx->perms.as<uint8_t>(), st));
     a.fk_perm = K == 1 ? ctx->perms.as<uint8_t>() : nullptr;
     BCC_CUDA(ctx, ops->prep(a, st));  // records stage events 1-4
-    a.mode = K == 1 ? 0 : 4;
+    a.mode = K == 1 ? a.mode : 4;  // one cluster: the plain walk (whole or half warp) over the permuted table
     BCC_CUDA(ctx, ops->check_mode(a, st));
     if (ev) cudaEventRecord(ev[5], st);
     return BCC_OK;
@@ -404,7 +405,7 @@ bcc_status launch_sequence(bcc_ctx* ctx, bcc_robot robot, bcc::PipelineArgs& a, 
 bool same_tune(const bcc::Tune& x, const bcc::Tune& y) {
     return x.edges_per_cta == y.edges_per_cta && x.warps == y.warps && x.persistent == y.persistent &&
            x.queue_min_items == y.queue_min_items && x.finish_split == y.finish_split &&
-           x.learned_mode == y.learned_mode && x.clusters == y.clusters;
+           x.learned_mode == y.learned_mode && x.clusters == y.clusters && x.lanes == y.lanes;
 }
 
 bcc_status run_check(bcc_ctx* ctx, bcc_robot robot, const float* d_edges, int E, int resolution,
@@ -797,6 +798,7 @@ bcc_status bcc_check(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32_t 
     BCC_CUDA(ctx, cudaStreamSynchronize(st));
     int flag = 0;
     BCC_CUDA(ctx, cudaMemcpy(&flag, ctx->error_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag & 4) return fail(ctx, BCC_ERR_TIMEOUT, "a walk exceeded its step bound");
     if (flag) return fail(ctx, BCC_ERR_TIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
     return BCC_OK;
 }
@@ -1156,7 +1158,8 @@ int64_t bcc_last_learned_pairs(const bcc_ctx* ctx) {
 // [1] warps per CTA, [2] persistent kernel (0/1), [3] learned-order queue
 // threshold (items), [4] learned-order finish: 1 = each queued pair split over
 // a CTA's warps, 0 = one warp per pair, [5] learned order: 0 = inline, 1 =
-// queued, [6] inline learned order: environment clusters (1..64).
+// queued, [6] inline learned order: environment clusters (1..64), [7] lanes
+// per walking pair in the plain-order walk (32, or 16: half-warps).
 bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg) {
     if (!ctx || !cfg) return BCC_ERR_INVALID_ARGUMENT;
     cfg[0] = ctx->tune.edges_per_cta;
@@ -1166,6 +1169,7 @@ bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg) {
     cfg[4] = ctx->tune.finish_split;
     cfg[5] = ctx->tune.learned_mode;
     cfg[6] = ctx->tune.clusters;
+    cfg[7] = ctx->tune.lanes;
     return BCC_OK;
 }
 
@@ -1173,7 +1177,7 @@ bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg) {
     if (!ctx || !cfg) return BCC_ERR_INVALID_ARGUMENT;
     if (cfg[0] < 1 || cfg[0] > 4096 || (cfg[1] != 1 && cfg[1] != 2 && cfg[1] != 4 && cfg[1] != 8) ||
         (cfg[2] != 0 && cfg[2] != 1) || cfg[3] < 0 || (cfg[4] != 0 && cfg[4] != 1) ||
-        (cfg[5] != 0 && cfg[5] != 1) || cfg[6] < 1 || cfg[6] > 64)
+        (cfg[5] != 0 && cfg[5] != 1) || cfg[6] < 1 || cfg[6] > 64 || (cfg[7] != 32 && cfg[7] != 16))
         return fail(ctx, BCC_ERR_INVALID_ARGUMENT, "bad launch configuration");
     ctx->tune.edges_per_cta = cfg[0];
     ctx->tune.warps = cfg[1];
@@ -1182,6 +1186,7 @@ bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg) {
     ctx->tune.finish_split = cfg[4];
     ctx->tune.learned_mode = cfg[5];
     ctx->tune.clusters = cfg[6];
+    ctx->tune.lanes = cfg[7];
     return BCC_OK;
 }
 
@@ -1267,16 +1272,19 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
     // Launch shape first (for the learned order at a middle threshold with
     // one-warp finishes), then the learned order's threshold x finish mode at
     // that shape, then the shape once more at the chosen threshold and mode.
+    const int lanes[2] = {32, 16};
     auto sweep_shape = [&](const bcc::Tune& from) {
         for (int ti = 0; ti < 4 && s == BCC_OK; ++ti)
             for (int wi = 0; wi < 2 && s == BCC_OK; ++wi)
-                for (int pe = 0; pe < 2 && s == BCC_OK; ++pe) {
-                    bcc::Tune t = from;
-                    t.edges_per_cta = tiles[ti];
-                    t.warps = warps[wi];
-                    t.persistent = pe;
-                    keep(t);
-                }
+                for (int pe = 0; pe < 2 && s == BCC_OK; ++pe)
+                    for (int li = 0; li < 2 && s == BCC_OK; ++li) {
+                        bcc::Tune t = from;
+                        t.edges_per_cta = tiles[ti];
+                        t.warps = warps[wi];
+                        t.persistent = pe;
+                        t.lanes = lanes[li];
+                        keep(t);
+                    }
     };
     bcc::Tune start = base;
     if (learned) {  // the inline order at one cluster while the shape is swept

@@ -53,6 +53,7 @@ struct Tune {
     int finish_split = 0;    // learned order, queued: 1 = split each queued pair over a CTA's warps
     int learned_mode = 0;    // learned order: 0 = inline (per-cluster scores), 1 = queued (per-pair scores)
     int clusters = 1;        // learned order, inline: environment clusters scored per edge
+    int lanes = 32;          // lanes per walking pair in the plain-order walk: 32 or 16 (half-warps)
     bool tuned = false;
 };
 

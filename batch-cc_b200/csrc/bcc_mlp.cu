@@ -50,8 +50,9 @@ constexpr uint32_t kImagesBytes = kImagesW + 3 * kImgSmall;  // ... | W4 | B2 | 
 constexpr int kBiasCol = kMlpIn - 1;                        // feature 47: reserved, read as 1 by the forward kernel
 
 // Shared-memory map of the forward kernel (bytes): the images, the ones image
-// (A operand of the bias MMAs), then per row group its X tile (128 x 48) and H
-// tile (128 x 128), b4, the groups' mbarriers and the TMEM address slot.
+// (A operand of the bias MMAs), then per row group one buffer for its X tile
+// (128 x 48) and, once the first MMA has consumed X, its H tile (128 x 128),
+// b4, the groups' mbarriers and the TMEM address slot.
 constexpr uint32_t kSmW1 = 0;
 constexpr uint32_t kSmW2 = kSmW1 + kImgW1;
 constexpr uint32_t kSmW3 = kSmW2 + kImgW;
@@ -59,10 +60,12 @@ constexpr uint32_t kSmW4 = kSmW3 + kImgW;
 constexpr uint32_t kSmB2 = kSmW4 + kImgSmall;
 constexpr uint32_t kSmB3 = kSmB2 + kImgSmall;
 constexpr uint32_t kSmOnes = kSmB3 + kImgSmall;
-constexpr int kFwdGroups = 3;                              // independent 128-row tile streams per CTA
+constexpr int kFwdGroups = 4;                              // independent 128-row tile streams per CTA
 constexpr uint32_t kFwdTmemCols = 512;                     // power of two >= 128 x groups
-constexpr uint32_t kSmGroup0 = kSmOnes + kImgSmall;        // group g: X at +g*stride, H at +kImgW1
-constexpr uint32_t kSmGroupStride = kImgW1 + kImgW;
+// Group g's buffer at kSmGroup0 + g * stride holds its X tile (128 x 48) until
+// the first layer's MMA has read it, then its H tile (128 x 128).
+constexpr uint32_t kSmGroup0 = kSmOnes + kImgSmall;
+constexpr uint32_t kSmGroupStride = kImgW;
 constexpr uint32_t kSmVec = kSmGroup0 + kFwdGroups * kSmGroupStride;  // b4
 constexpr uint32_t kSmBar = kSmVec + 16;
 constexpr uint32_t kSmTmem = kSmBar + 8 * kFwdGroups;
@@ -185,10 +188,10 @@ __device__ __forceinline__ bool group_sync_or(bool pred, int grp) {
     return r != 0;
 }
 
-// Persistent: each CTA loads the weights once; its three warp groups (4 warps,
+// Persistent: each CTA loads the weights once; its four warp groups (4 warps,
 // one row per thread each) run independent streams of 128-row tiles, each with
-// its own X/H images, TMEM accumulator (columns 128 g ..) and mbarrier, so one
-// group's MMAs overlap the others' epilogues.  The biases ride in the MMAs (b1
+// its own X/H buffer, TMEM accumulator (columns 128 g ..) and mbarrier, so one
+// group's MMAs overlap the others' epilogues (all 512 TMEM columns in use).  The biases ride in the MMAs (b1
 // as column 47 of W1^T against feature 47 read as 1; b2, b3 by a K = 16 MMA of
 // a ones column against B2 / B3) and the output layer is an N = 16 MMA against
 // W4, so each hidden epilogue is only ReLU + BF16 conversion + store.  x: BF16
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 1)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kSmTmem);
     float* vec = reinterpret_cast<float*>(sm + kSmVec);
     uint8_t* xs = sm + kSmGroup0 + grp * kSmGroupStride;
-    uint8_t* hs = xs + kImgW1;
+    uint8_t* hs = xs;  // H overwrites X once the first layer's MMA has read it
 
     for (uint32_t i = t; i < kImagesBytes / 16; i += blockDim.x) reinterpret_cast<uint4*>(sm)[i] = images[i];
     if (t < 128) {  // ones image [128][16]: column 0 = 1 (BF16 0x3f80), the rest 0

@@ -951,6 +951,155 @@ __device__ __forceinline__ void walk_listed_pair(const CheckParams& P, int env, 
     }
 }
 
+// Plain order with 16 lanes per walking pair (MODE 5; robots whose leaves lie
+// inside their bounds): the warp's two halves walk two listed pairs at once,
+// 16 (sample rank, candidate) items a step each, in the reference's order.
+// The leaf work of a step is flattened inside each half; a half whose pair is
+// decided (a hit, or every item walked) writes the verdict and takes the next
+// pair of the walk list wt[0 .. nwalk).  A pair that collides in its first 16
+// items -- most of them -- then costs half a warp step instead of a whole one.
+template <class M, int SUB>
+__device__ __forceinline__ void walk_halves(const CheckParams& P, int env, int e0, int nwalk, const int (&wt)[SUB],
+                                            const int (&Cs)[SUB], const int (&base)[SUB], const uint16_t* pairs,
+                                            const float4* prim, const GroupLanes& GL) {
+    static_assert(!has_overhang<M>(), "the half-warp walk covers robots whose leaves lie inside their bounds");
+    constexpr int G = M::num_env_groups;
+    constexpr int GB = group_bits<M>();
+    constexpr int H = 16;
+    const int lane = threadIdx.x & 31, h = lane >> 4, hl = lane & (H - 1);
+    const unsigned hmask = h ? 0xffff0000u : 0x0000ffffu;
+    int t = -1, C = 1, bse = 0, n = 1, total = 0, w0 = 0, r = 0, c = 0, dr = 0, dc = 0, e = e0, row0 = 0;
+    WalkStats st;
+    auto take = [&](int idx) {
+        int tt = -1;
+#pragma unroll
+        for (int u = 0; u < SUB; ++u)
+            if (u == idx && u < nwalk) tt = wt[u];
+        t = tt;
+        if (t >= 0) {
+            int cc = 1, bb = 0;
+#pragma unroll
+            for (int u = 0; u < SUB; ++u)
+                if (u == t) {
+                    cc = Cs[u];
+                    bb = base[u];
+                }
+            C = cc;
+            bse = bb;
+            e = e0 + t;
+            n = P.steps[e];
+            row0 = P.offs[e];
+            total = kLanes * n * C;
+            w0 = 0;
+            // a / C for a <= 16 in FP32, exact as in walk_pairs
+            const float inv_c = __frcp_rn((float)C);
+            dr = (int)(16.5f * inv_c);
+            dc = H - dr * C;
+            r = (int)(((float)hl + 0.5f) * inv_c);
+            c = hl - r * C;
+            st = WalkStats();
+        }
+    };
+    take(h);
+    int nxt = 2;
+    // Bound on the loop (the warp-uniform step count): every step walks 16
+    // items of each live pair or ends one, so a group of pairs needs far fewer;
+    // past it the warp flags the error and leaves.
+    unsigned steps_left = 1u << 24;
+    for (;;) {
+        const bool act = t >= 0;
+        if (!__any_sync(kFull, act)) break;
+        if (--steps_left == 0) {
+            if (lane == 0) atomicOr(P.error_flag, 4);
+            break;
+        }
+        const uint32_t pr = act ? (uint32_t)pairs[bse + c] : 0u;
+        const int g = (int)(pr & ((1u << GB) - 1u));
+        const int p = (int)(pr >> GB);
+        const int fc = __shfl_sync(kFull, GL.fc, g);
+        const int first = fc & 0xffff, gcnt = fc >> 16;
+        int k = 0, cnt = 0;
+        if (act && w0 + hl < total) {
+            k = reference_rank_to_sample(r, n);
+            float4 bs = P.table[table_index<M>((size_t)(row0 + k), g)];
+            bs.w += kEnvInflate;
+            cnt = sphere_hits_prim(bs, prim + p * kPrimF4) ? gcnt : 0;
+        }
+        if (act) ++st.chunks;
+        bool hitp = false;
+        const unsigned gates = __ballot_sync(kFull, cnt > 0);
+        if (gates) {
+            if (gates & hmask) ++st.gates;
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < H; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, incl, o, H);
+                if (hl >= o) incl += y;
+            }
+            const int L = __shfl_sync(kFull, incl, H - 1, H);
+            const int Lw = max(L, __shfl_xor_sync(kFull, L, 16));
+            // a slot's item: its sample, primitive and leaf offset (first - exclusive count)
+            static_assert(max_prims_of<M>() < 4096, "primitive index packs into 12 bits");
+            const int dp = (int)(((unsigned)(first - (incl - cnt)) << 12) | (unsigned)p);
+            for (int t0 = 0; t0 < Lw; t0 += H) {
+                const int tt = t0 + hl;
+                int j = 0;  // owner: the first lane of the half whose inclusive count exceeds tt
+#pragma unroll
+                for (int step = H / 2; step; step >>= 1) {
+                    const int v = __shfl_sync(kFull, incl, j + step - 1, H);
+                    if (v <= tt) j += step;
+                }
+                const int jd = __shfl_sync(kFull, dp, j, H);
+                const int jk = __shfl_sync(kFull, k, j, H);
+                bool hit = false;
+                if (tt < L) {
+                    float4 ls = P.table[table_index<M>((size_t)(row0 + jk), G + tt + (jd >> 12))];
+                    ls.w += kEnvInflate;
+                    hit = sphere_hits_prim(ls, prim + (jd & 4095) * kPrimF4);
+                }
+                if (t0 < L) ++st.leaf;
+                // the ballot on its own statement: every lane must reach it, so it
+                // must not sit behind a short-circuiting ||
+                const unsigned hb = __ballot_sync(kFull, hit);
+                hitp = hitp || (hb & hmask) != 0;
+                if (__all_sync(kFull, hitp || t0 + H >= L)) break;  // every half hit or out of slots
+            }
+        }
+        bool fin = false;
+        if (act) {
+            if (hitp) {
+                fin = true;
+            } else {
+                w0 += H;
+                c += dc;
+                r += dr;
+                if (c >= C) {
+                    c -= C;
+                    ++r;
+                }
+                fin = w0 >= total;
+            }
+        }
+        if (fin && hl == 0) {
+            P.results[(size_t)e * P.num_envs + env] = hitp ? 1 : 0;
+            if (P.counters) {
+                atomicAdd(P.counters + 0, 1ull);
+                atomicAdd(P.counters + 1, (unsigned long long)C);
+                atomicAdd(P.counters + 2, st.chunks);
+                atomicAdd(P.counters + 3, st.gates);
+                atomicAdd(P.counters + 4, st.leaf);
+                atomicAdd(P.counters + 5, hitp ? 1ull : 0ull);
+            }
+        }
+        // next pairs, in half order, the same on every lane
+        const unsigned fb = __ballot_sync(kFull, fin && hl == 0);
+        const int f0 = (int)(fb & 1u), f1 = (int)((fb >> 16) & 1u);
+        const int i0 = nxt, i1 = nxt + f0;
+        nxt += f0 + f1;
+        if (fin) take(h ? i1 : i0);
+    }
+}
+
 // Pairs (env, e0 .. e0 + count - 1), count <= pairs_per_setup<M>(), whole
 // warp: lane group s = lane / G culls pair s (lane g of the group ANDs link
 // g's three masks), a scan inside each group gives every link its offset,
@@ -995,9 +1144,10 @@ __device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, 
         base[t] = total;
         total += t < count ? Cs[t] : 0;
     }
+    constexpr int PAIR_MODE = MODE == 5 ? 0 : MODE;
     if (total > P.pairs_per_warp) {
         for (int t = 0; t < count; ++t)
-            check_pair<M, MODE>(P, env, e0 + t, -1, prim, masks, np, W, pairs, nullptr, GL);
+            check_pair<M, PAIR_MODE>(P, env, e0 + t, -1, prim, masks, np, W, pairs, nullptr, GL);
         return;
     }
     if (cnt > 0) {
@@ -1015,6 +1165,35 @@ __device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, 
         }
     }
     __syncwarp();
+    if constexpr (MODE == 5) {
+        // the pairs decided without a walk first, the rest walked by half-warps
+        int wt[SUB];
+        int nwalk = 0;
+#pragma unroll
+        for (int t = 0; t < SUB; ++t) wt[t] = -1;
+#pragma unroll
+        for (int t = 0; t < SUB; ++t) {
+            if (t >= count) continue;  // warp-uniform
+            const int et = e0 + t;
+            const int self_t = __shfl_sync(kFull, self, t * G);
+            if (np == 0 || self_t) {
+                if (lane == 0) P.results[(size_t)et * P.num_envs + env] = self_t ? 1 : 0;
+                continue;
+            }
+            if (Cs[t] == 0) {
+                if (lane == 0) {
+                    P.results[(size_t)et * P.num_envs + env] = 0;
+                    if (P.counters) atomicAdd(P.counters + 0, 1ull);
+                }
+                continue;
+            }
+#pragma unroll
+            for (int u = 0; u < SUB; ++u)
+                if (u == nwalk) wt[u] = t;
+            ++nwalk;
+        }
+        walk_halves<M, SUB>(P, env, e0, nwalk, wt, Cs, base, pairs, prim, GL);
+    } else {
 #pragma unroll 1
     for (int t = 0; t < count; ++t) {
         const int et = e0 + t;
@@ -1035,6 +1214,7 @@ __device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, 
         for (int u = 0; u < SUB; ++u)
             if (u == t) bt = base[u];
         walk_listed_pair<M, MODE>(P, env, et, Cs[t], pairs + bt, prim, np, GL);
+    }
     }
     __syncwarp();  // every lane is done with the lists before the next group's writes
 }
@@ -1689,6 +1869,9 @@ cudaError_t launch_check_w(CheckParams P, int E, cudaStream_t st, int mode) {
         case 1: return launch_check_wm<M, W, 1>(P, E, st);
         case 2: return launch_finish_w<M, W>(P, st);
         case 4: return launch_check_wm<M, W, 4>(P, E, st);
+        case 5:  // 16 lanes per walking pair, where the robot has a grouped cull and no overhang
+            if constexpr (!has_overhang<M>() && pairs_per_setup<M>() > 1) return launch_check_wm<M, W, 5>(P, E, st);
+            return launch_check_wm<M, W, 0>(P, E, st);
         default: return launch_check_wm<M, W, 0>(P, E, st);
     }
 }

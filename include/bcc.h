@@ -146,8 +146,9 @@ int32_t bcc_stage_times(bcc_ctx* ctx, float* ms, int32_t max_stages);
 /*
  * Work counters of the last check, when profiling was switched on with bit 1
  * set (bcc_set_profiling(ctx, 3)): [0] pairs walked, [1] candidate
- * (primitive, link) pairs after the cull, [2] 32-item chunks, [3] chunks with a
- * gate hit, [4] leaf steps, [5] colliding pairs.  Diagnostics only: counting
+ * (primitive, link) pairs after the cull, [2] walk steps (32 items, or 16
+ * with 16 lanes per walking pair), [3] steps with a gate hit, [4] leaf steps,
+ * [5] colliding pairs.  Diagnostics only: counting
  * adds atomics to the check kernel.  Returns the number written, or -1.
  */
 int32_t bcc_work_counters(bcc_ctx* ctx, uint64_t* out, int32_t max_counters);
@@ -284,14 +285,18 @@ bcc_status bcc_measure_fp32_peak(int32_t device, double* tflops);
  * cluster, in one pass), 1 = queued (pairs left undecided by a plain probe of
  * their first sample are scored per pair and finished in a second pass),
  * cfg[6] inline order: environment clusters, 1..64 (k-means over the
- * environment codes; the MLP scores each edge's segments once per cluster).
+ * environment codes; the MLP scores each edge's segments once per cluster),
+ * cfg[7] lanes per walking pair in the plain-order walk: 32 (a whole warp) or
+ * 16 (the warp's halves walk two pairs at once, 16 items a step each; robots
+ * whose leaves lie inside their bounds, otherwise 32 is used).
  */
-#define BCC_LAUNCH_CONFIG_LEN 7
+#define BCC_LAUNCH_CONFIG_LEN 8
 bcc_status bcc_get_launch_config(const bcc_ctx* ctx, int32_t* cfg);
 bcc_status bcc_set_launch_config(bcc_ctx* ctx, const int32_t* cfg);
 /*
  * Autotuner: times candidate configurations (edges per CTA 32..256, 4 or 8
- * warps, persistent or not; for the learned order also the inline order's
+ * warps, persistent or not, 32 or 16 lanes per walking pair; for the learned
+ * order also the inline order's
  * cluster count and the queued order's threshold 64..4096 items and finish
  * mode) on the given host edges against the
  * uploaded environments, timing graph replays, and keeps the fastest in the
