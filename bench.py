@@ -531,11 +531,22 @@ def run_ours(args, world, rank, local, dist):
         dist.barrier()
     torch.cuda.synchronize()
     results = {}
+    # Timed region: both orders, then the learned pipeline once more with the
+    # network at its seeded initialisation (what the training itself adds),
+    # each under the same clocks, launch and L2 flushes.
+    from bcc import mlp as _mlp
+    trained_params = chk.mlp_get_params()
     with ClockSampler(dev) as clk:
         for order in ("plain", "learned"):
             chk.set_launch_config(**tuned[order])
             results[order] = time_order(chk, d_edges, d_res, E, order, stream, args.steps, args.warmup, flush, dev,
                                         robot)
+        chk.mlp_set_params(_mlp.init_params(1000))
+        chk.set_launch_config(**tuned["learned"])
+        untrained_ms = max_over_ranks(dist, time_order(chk, d_edges, d_res, E, "learned", stream, args.steps,
+                                                       args.warmup, flush, dev, robot, eager_reps=0)[0],
+                                      f"cuda:{dev}") / args.steps
+        chk.mlp_set_params(trained_params)
     torch.cuda.synchronize()
 
     ms = {o: max_over_ranks(dist, results[o][0], f"cuda:{dev}") / args.steps for o in results}
@@ -560,11 +571,7 @@ def run_ours(args, world, rank, local, dist):
         c = chk.work_counters()
         work[order] = {k: v / max(c["pairs"], 1) for k, v in c.items() if k != "pairs"}
         work[order]["pairs_walked"] = c["pairs"]
-    # What the training adds: the same learned pipeline and launch with the
-    # network at its seeded initialisation (untrained), timed the same way,
-    # and its work counters.
-    from bcc import mlp as _mlp
-    trained_params = chk.mlp_get_params()
+    # work counters of the untrained network's learned order (the ablation)
     chk.mlp_set_params(_mlp.init_params(1000))
     chk.set_launch_config(**tuned["learned"])
     chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream, robot=robot)
@@ -572,8 +579,6 @@ def run_ours(args, world, rank, local, dist):
     c = chk.work_counters()
     work_untrained = {k: v / max(c["pairs"], 1) for k, v in c.items() if k != "pairs"}
     chk.set_profiling(True)
-    untrained_ms = time_order(chk, d_edges, d_res, E, "learned", stream, args.steps, args.warmup, flush, dev, robot,
-                              eager_reps=0)[0] / args.steps
     chk.mlp_set_params(trained_params)
     chk.check_device(d_edges.data_ptr(), E, d_res.data_ptr(), order="learned", stream=stream.cuda_stream, robot=robot)
     torch.cuda.synchronize()
@@ -618,7 +623,7 @@ def run_ours(args, world, rank, local, dist):
             "verdict_mismatches_learned_vs_plain": mismatch,
             "proposal": dict(proposal, scored_segments_per_step=learned_rows, queued_pairs_per_step=learned_pairs,
                              queued_fraction=learned_pairs / float(N * E), ranking=ranking),
-            "gpu_launches": (6 + 9) * args.steps,  # plain: 6 launches per step; learned: 9
+            "gpu_launches": (6 + 9 + 9) * args.steps,  # plain: 6 launches per step; learned and its ablation: 9
             "clocks": clk.summary()}
     line["e2e"] = {"value": world * N * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(edges.nbytes),
                    "d2h_bytes_per_step": int(N * E),
