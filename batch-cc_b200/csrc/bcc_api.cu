@@ -1272,12 +1272,16 @@ bcc_status bcc_autotune(bcc_ctx* ctx, bcc_robot robot, const float* edges, int32
     // Launch shape first (for the learned order at a middle threshold with
     // one-warp finishes), then the learned order's threshold x finish mode at
     // that shape, then the shape once more at the chosen threshold and mode.
+    // Lanes per walking pair: 16 only where the robot has the half-warp walk
+    // (elsewhere it would time the 32-lane walk twice and could report 16).
     const int lanes[2] = {32, 16};
+    const bcc::RobotOps* tops = bcc::robot_ops((int)robot);
+    const int n_lanes = tops && tops->half_warp_walk ? 2 : 1;
     auto sweep_shape = [&](const bcc::Tune& from) {
         for (int ti = 0; ti < 4 && s == BCC_OK; ++ti)
             for (int wi = 0; wi < 2 && s == BCC_OK; ++wi)
                 for (int pe = 0; pe < 2 && s == BCC_OK; ++pe)
-                    for (int li = 0; li < 2 && s == BCC_OK; ++li) {
+                    for (int li = 0; li < n_lanes && s == BCC_OK; ++li) {
                         bcc::Tune t = from;
                         t.edges_per_cta = tiles[ti];
                         t.warps = warps[wi];

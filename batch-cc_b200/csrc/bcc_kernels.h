@@ -146,6 +146,7 @@ struct RobotOps {
     int num_spheres;         // sample-table row width (float4 per sample)
     int num_env_groups;
     int max_prims;           // primitives per environment the pair packing allows
+    bool half_warp_walk;     // the 16-lane walk exists (no overhang, grouped cull); else lanes 16 walks as 32
     cudaError_t (*upload_tables)();  // robot tables -> __constant__ of the current device
     // Stage 1: steps + sample offsets (total rows land in offs[E]).
     cudaError_t (*steps)(const PipelineArgs& a, cudaStream_t st);

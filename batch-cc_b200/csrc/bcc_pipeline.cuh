@@ -2007,6 +2007,7 @@ RobotOps robot_ops_of(int robot, cudaError_t (*upload)()) {
     o.num_spheres = M::num_spheres;
     o.num_env_groups = M::num_env_groups;
     o.max_prims = max_prims_of<M>();
+    o.half_warp_walk = !has_overhang<M>() && pairs_per_setup<M>() > 1;
     o.upload_tables = upload;
     o.steps = run_steps<M>;
     o.check = run_check<M>;
