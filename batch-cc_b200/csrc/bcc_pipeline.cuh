@@ -1507,10 +1507,18 @@ __global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finis
 
 // ------------------------------------------------------------------ learned order
 // One MLP feature row: joints normalised to [-1, 1] by the joint limits, the
-// environment code, zeros; BF16, kMlpIn values.
+// environment code, zeros, and in column kMlpIn - 2 the sample's position
+// along its edge (sample k of 32 n mapped to [-1, 1]: where on an edge whose
+// start is free a collision lies is the strongest per-sample signal the
+// walk order can use); column kMlpIn - 1 stays zero (the forward kernel's bias
+// input).  BF16, kMlpIn values.
+__device__ __forceinline__ float sample_position(int k, int n) {
+    return 2.0f * (float)k / (float)(kLanes * n - 1) - 1.0f;
+}
+
 template <class M>
-__device__ __forceinline__ void write_features(const float* q, const float* code, uint16_t* dst) {
-    static_assert(M::dof + kEnvCode <= kMlpIn, "feature row too narrow for this robot");
+__device__ __forceinline__ void write_features(const float* q, const float* code, float pos, uint16_t* dst) {
+    static_assert(M::dof + kEnvCode <= kMlpIn - 2, "feature row too narrow for this robot");
     const DevTables<M>& T = tab<M>();
     float f[kMlpIn];
 #pragma unroll
@@ -1519,6 +1527,7 @@ __device__ __forceinline__ void write_features(const float* q, const float* code
     for (int j = 0; j < M::dof; ++j) f[j] = 2.0f * (q[j] - T.s_a[j]) / T.s_m[j] - 1.0f;
 #pragma unroll
     for (int j = 0; j < kEnvCode; ++j) f[M::dof + j] = code[j];
+    f[kMlpIn - 2] = pos;
     uint32_t w[kMlpIn / 2];
 #pragma unroll
     for (int j = 0; j < kMlpIn / 2; ++j) {
@@ -1558,8 +1567,9 @@ __global__ void queue_features_kernel(CheckParams P, const float* __restrict__ e
             t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
         }
         for (int seg = sl; seg < 4 * n; seg += kFeatureLanes) {
-            edge_sample<M::dof>(s, t, n, seg * kSegment + kSegment - 1, q);
-            write_features<M>(q, code + (size_t)env * kEnvCode, x + (size_t)(ro + seg) * kMlpIn);
+            const int k = seg * kSegment + kSegment - 1;
+            edge_sample<M::dof>(s, t, n, k, q);
+            write_features<M>(q, code + (size_t)env * kEnvCode, sample_position(k, n), x + (size_t)(ro + seg) * kMlpIn);
         }
     }
 }
@@ -1593,8 +1603,9 @@ __global__ void cluster_features_kernel(CheckParams P, const float* __restrict__
         s[d] = edges[(size_t)e * 2 * M::dof + d];
         t[d] = edges[(size_t)e * 2 * M::dof + M::dof + d];
     }
-    edge_sample<M::dof>(s, t, P.steps[e], j * kSegment + kSegment - 1, q);
-    write_features<M>(q, centroids + (size_t)c * kEnvCode, x + (size_t)i * kMlpIn);
+    const int k = j * kSegment + kSegment - 1;
+    edge_sample<M::dof>(s, t, P.steps[e], k, q);
+    write_features<M>(q, centroids + (size_t)c * kEnvCode, sample_position(k, P.steps[e]), x + (size_t)i * kMlpIn);
 }
 
 // Inline learned order, permutations: one warp per (cluster c, edge e).
@@ -1705,7 +1716,7 @@ __global__ void training_rows_kernel(CheckParams P, const float* __restrict__ ed
         t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
     }
     edge_sample<M::dof>(s, t, n, k, q);
-    write_features<M>(q, code + (size_t)env * kEnvCode, x + (size_t)i * kMlpIn);
+    write_features<M>(q, code + (size_t)env * kEnvCode, sample_position(k, n), x + (size_t)i * kMlpIn);
     y[i] = sample_hits_env<M>(P, env, (size_t)P.offs[e] + k) ? 1 : 0;
 }
 

@@ -287,3 +287,46 @@ def test_ordering_can_save_little_on_the_uneven_workload():
             plain, perfect = plain + 32 * n, perfect + 32 * n
     assert colliding > 100 and rank0 / colliding > 0.9
     assert 1.0 - perfect / plain < 0.15
+
+
+def _ranks_walked(hits, n, pi):
+    """Ranks a walk visits per pair when rank r checks sample pi[r % 32] * n + r // 32
+    (pi = identity is the reference order, src/batch_cc.cu:118-129): up to and
+    including the first colliding one, or all 32 n for a collision-free pair."""
+    r = np.arange(32 * n)
+    h = hits[:, pi[r % 32] * n + r // 32]
+    return np.where(h.any(1), np.argmax(h, 1) + 1, 32 * n)
+
+
+def test_per_edge_order_ceiling_on_the_uneven_workload():
+    """What any scorer of an edge's 32 lane blocks can gain over a random block
+    order (block 0 first) on the uneven workload: the exact per-sample verdicts
+    of 100 000 (edge, env) pairs give, per edge, the greedy block order built
+    from the answers themselves (an upper bound for a scorer that sees only the
+    edge, as the one-cluster learned order does).  It beats the random order by
+    a few percent of the walked ranks, while the random order already takes most
+    of the per-pair perfect order's saving: the structure of the order matters
+    more than the scores on this workload."""
+    E, N = 1000, 100
+    envs = workload.gen_envs("uneven", N, seed=0)
+    edges = workload.gen_edges("uneven", E, seed=0)
+    pairs = np.array([(e, v) for e in range(E) for v in range(N)], np.int64)
+    S = orc.pair_samples(envs, edges, pairs) == 1
+    ns = np.array([orc.edge_n(edges[e, 0], edges[e, 1], 32) for e in range(E)])
+    rng = np.random.default_rng(0)
+    tot = {"plain": 0, "random": 0, "reverse": 0, "per_edge_best": 0, "per_pair_perfect": 0}
+    for e in range(E):
+        n, h = int(ns[e]), S[e * N:(e + 1) * N]
+        tot["plain"] += _ranks_walked(h, n, np.arange(32)).sum()
+        tot["random"] += _ranks_walked(h, n, np.concatenate([[0], 1 + rng.permutation(31)])).sum()
+        tot["reverse"] += _ranks_walked(h, n, np.concatenate([[0], np.arange(31, 0, -1)])).sum()
+        alive, order, rest = ~h[:, 0], [0], list(range(1, 32))
+        while rest:  # greedy: the block whose first sample decides most undecided pairs
+            b = max(rest, key=lambda b: (h[alive, b * n].sum(), -b))
+            order.append(b); rest.remove(b); alive &= ~h[:, b * n]
+        tot["per_edge_best"] += _ranks_walked(h, n, np.array(order)).sum()
+        tot["per_pair_perfect"] += np.where(h.any(1), 1, 32 * n).sum()
+    save = {k: 1.0 - v / tot["plain"] for k, v in tot.items()}
+    assert 0 < save["random"] < save["per_edge_best"] <= save["per_pair_perfect"] < 0.15
+    assert save["per_edge_best"] - save["random"] < 0.04
+    assert save["random"] > 0.6 * save["per_pair_perfect"]
