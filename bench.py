@@ -330,7 +330,8 @@ def train_proposal(chk, args):
     t0 = time.perf_counter()
     chk.upload(workload.gen_envs(args.workload, args.train_envs, seed=1000))
     chk.mlp_set_params(mlp.init_params(1000))
-    losses, pos, rows = chk.mlp_train_queued(workload.gen_edges(args.workload, args.edges, seed=1000),
+    train_edges = workload.gen_edges(args.workload, args.edges, seed=1000)
+    losses, pos, rows = chk.mlp_train_queued(train_edges,
                                              num_samples=args.train_samples, queue_min_items=TRAIN_QUEUE_MIN_ITEMS,
                                              epochs=args.train_epochs, batch=16384, lr=2e-3, seed=1000,
                                              robot=workload.robot_of(args.workload))
@@ -338,7 +339,7 @@ def train_proposal(chk, args):
             "train_positive_fraction": pos, "train_seconds": time.perf_counter() - t0,
             "data": "segments (scored at their last sample) of the pairs the probe queues at threshold %d, "
                     "checker-labelled, %d %s environments x %d edges with seed 1000 (benchmark uses seed 0)" % (
-                        TRAIN_QUEUE_MIN_ITEMS, args.train_envs, args.workload, args.edges or 0)}
+                        TRAIN_QUEUE_MIN_ITEMS, args.train_envs, args.workload, len(train_edges))}
 
 
 def proposal_ranking(chk, edges, queue_min_items, robot):

@@ -148,6 +148,34 @@ def test_work_counters_of_both_networks(checker, trained):
     assert work["trained"]["pairs"] == work["untrained"]["pairs"]
 
 
+def test_trained_inline_order_walks_fewer_chunks(checker, trained):
+    """What the learning adds to the order the tuner picks (inline, one
+    cluster), on held-out environments and edges: the walk with the trained
+    network takes fewer 32-item chunks per pair than with an untrained network
+    (the order's structure alone), which takes fewer than the plain order."""
+    envs = workload.gen_envs("uneven", 200, seed=31)
+    edges = workload.gen_edges("uneven", 3000, seed=31)
+    checker.upload(envs)
+    cfg = checker.launch_config()
+    checker.set_launch_config(learned_mode=0, clusters=1)
+    checker.set_profiling(True, counters=True)
+    chunks, verdicts = {}, {}
+    try:
+        verdicts["plain"] = checker.check(edges, order="plain")
+        chunks["plain"] = checker.work_counters()["chunks"]
+        for label, params in (("untrained", mlp.init_params(99)), ("trained", trained["params"])):
+            checker.mlp_set_params(params)
+            verdicts[label] = checker.check(edges, order="learned")
+            chunks[label] = checker.work_counters()["chunks"]
+    finally:
+        checker.set_profiling(False)
+        checker.set_launch_config(**cfg)
+        checker.mlp_set_params(trained["params"])
+    assert np.array_equal(verdicts["trained"], verdicts["plain"])
+    assert np.array_equal(verdicts["untrained"], verdicts["plain"])
+    assert chunks["trained"] < chunks["untrained"] < chunks["plain"], chunks
+
+
 @pytest.mark.parametrize("row_cap", [3, 4, 64, 2000])
 @pytest.mark.parametrize("graph", [False, True])
 def test_row_budget_keeps_verdicts(checker, trained, learned_mode, row_cap, graph):
