@@ -183,64 +183,128 @@ __global__ void __launch_bounds__(128) fk_kernel(const float* __restrict__ edges
     row_edge[row] = e;
 }
 
-// Row-major tables (tile 1): a thread's row is 16 * num_spheres contiguous
-// bytes, so per-thread stores would touch 32 rows per warp instruction.  One
-// warp per CTA computes its 32 rows into shared memory (odd float4 row stride,
-// conflict-free) and then copies the 32 consecutive rows out as one contiguous
-// block, 512 bytes per warp store.
-template <class M>
-__global__ void __launch_bounds__(32) fk_staged_kernel(const float* __restrict__ edges, int E,
-                                                       const int* __restrict__ steps,
-                                                       const int* __restrict__ offs,
-                                                       float4* __restrict__ table,
-                                                       int* __restrict__ row_edge, const uint8_t* __restrict__ perm) {
-    static_assert(M::table_tile == 1, "row-major tables only");
-    constexpr int NS = M::num_spheres;
-    constexpr int STRIDE = NS | 1;
-    extern __shared__ float4 srow[];  // [32][STRIDE]
-    const int total = offs[E];
-    const int base = blockIdx.x * 32;
-    const int row = base + (int)threadIdx.x;
-    if (row < total) {
-        int lo = 0, hi = E - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (offs[mid] <= row) lo = mid; else hi = mid - 1;
-        }
-        const int e = lo;
-        const int k = row - offs[e];
-        float s[M::dof], t[M::dof], q[M::dof];
-#pragma unroll
-        for (int j = 0; j < M::dof; ++j) {
-            s[j] = edges[(size_t)e * 2 * M::dof + j];
-            t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
-        }
-        edge_sample<M::dof>(s, t, steps[e], table_sample(perm, e, steps[e], k), q);
-        fk_spheres<M>(q, srow + threadIdx.x * STRIDE);
-        row_edge[row] = e;
-    }
-    __syncwarp();
-    const int n = min(32, total - base) * NS;
-    float4* __restrict__ dst = table + (size_t)base * NS;
-    for (int i = threadIdx.x; i < n; i += 32) {
-        const int r = i / NS;
-        dst[i] = srow[r * STRIDE + (i - r * NS)];
-    }
-}
-
-// ------------------------------------------------------------------ 4. self
 __device__ __forceinline__ bool self_hit(float4 a, float4 b) {
     const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
     const float rs = a.w + b.w;
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) - rs * rs < 0.0f;
 }
 
-// One warp per sample row, rows strided over the grid.  Lanes test the self
-// groups' bound pairs 32 at a time; the leaf pairs of every group whose bound
-// pair hit are then tested 32 at a time (the reference's gate-then-leaves,
-// any hit = self-collision).  Rows of an edge already known to self-collide
-// are skipped.  The self tables are staged in shared memory: lanes read
-// different entries, which constant memory would serialise.
+// Self-collision of a warp's rows, one lane per row (sphere s at my[s]; live:
+// the lane holds a row), all rows of one edge: group g gates on its bound pair
+// and its leaf pairs count only where the gate hit (the reference's
+// gate-then-leaves).  The warp walks the groups together, so every table index
+// is warp-uniform (constant-cache broadcasts), skips a group's leaves when no
+// lane's gate hit, and stops at the first hit in any lane.  Warp-uniform.
+template <class M>
+__device__ __forceinline__ bool self_rows_hit(const float4* my, bool live) {
+    const DevTables<M>& T = tab<M>();
+    for (int g = 0; g < M::num_self_groups; ++g) {
+        const bool gate = live && self_hit(my[T.self_bound[g][0]], my[T.self_bound[g][1]]);
+        if (!__any_sync(kFull, gate)) continue;
+        bool h = false;
+        const int k1 = T.self_pair_begin[g + 1];
+#pragma unroll 4
+        for (int k = T.self_pair_begin[g]; k < k1; ++k) h |= self_hit(my[T.self_pairs[k][0]], my[T.self_pairs[k][1]]);
+        if (__any_sync(kFull, gate && h)) return true;
+    }
+    return false;
+}
+
+// Row-major tables (tile 1): a thread's row is 16 * num_spheres contiguous
+// bytes, so per-thread stores would touch 32 rows per warp instruction.  One
+// warp per CTA computes 32 rows into shared memory (odd float4 row stride,
+// conflict-free) and then copies the 32 consecutive rows out as one contiguous
+// block, 512 bytes per warp store.  While the rows are still in shared memory
+// the warp also runs their self-collision check, one lane per row, so the rows
+// are never read back from global memory for it.  A block's 32 rows belong to
+// one edge (every edge has 32 n rows and starts on a multiple of 32), so the
+// first hit in any lane decides the block.  The CTA strides over 32-row blocks.
+template <class M>
+__global__ void __launch_bounds__(32) fk_staged_kernel(const float* __restrict__ edges, int E,
+                                                       const int* __restrict__ steps,
+                                                       const int* __restrict__ offs,
+                                                       float4* __restrict__ table,
+                                                       int* __restrict__ row_edge, const uint8_t* __restrict__ perm,
+                                                       int* __restrict__ edge_self) {
+    static_assert(M::table_tile == 1, "row-major tables only");
+    constexpr int NS = M::num_spheres;
+    constexpr int STRIDE = NS | 1;
+    extern __shared__ float4 srow[];  // [32][STRIDE]
+    const int lane = threadIdx.x;
+    const int total = offs[E];
+    for (int base = blockIdx.x * 32; base < total; base += gridDim.x * 32) {
+        const int row = base + lane;
+        // the block's edge: the last e with offs[e] <= base (one search per block)
+        int lo = 0, hi = E - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (offs[mid] <= base) lo = mid; else hi = mid - 1;
+        }
+        const int e = lo;
+        const int n = steps[e];
+        if (row < total) {
+            float s[M::dof], t[M::dof], q[M::dof];
+#pragma unroll
+            for (int j = 0; j < M::dof; ++j) {
+                s[j] = edges[(size_t)e * 2 * M::dof + j];
+                t[j] = edges[(size_t)e * 2 * M::dof + M::dof + j];
+            }
+            edge_sample<M::dof>(s, t, n, table_sample(perm, e, n, row - offs[e]), q);
+            fk_spheres<M>(q, srow + lane * STRIDE);
+            row_edge[row] = e;
+        }
+        __syncwarp();
+        const int rows = min(32, total - base);
+        const int cnt = rows * NS;
+        float4* __restrict__ dst = table + (size_t)base * NS;
+        for (int i = lane; i < cnt; i += 32) {
+            const int r = i / NS;
+            dst[i] = srow[r * STRIDE + (i - r * NS)];
+        }
+        // self-collision of the block's rows (any hit marks the edge); skipped
+        // when another block of the edge has already marked it
+        int decided = lane == 0 ? *(volatile const int*)(edge_self + e) : 0;
+        if (!__shfl_sync(kFull, decided, 0) && self_rows_hit<M>(srow + lane * STRIDE, row < total) && lane == 0)
+            atomicOr(edge_self + e, 1);
+        __syncwarp();  // the next block overwrites srow
+    }
+}
+
+// ------------------------------------------------------------------ 4. self
+
+// Self-collision of one sample row, by one warp (sphere s at sp[s * stride]).
+// Lanes test the self groups' bound pairs 32 at a time; the leaf pairs of
+// every group whose bound pair hit are then tested 32 at a time (the
+// reference's gate-then-leaves, any hit = self-collision).  The tables are in
+// shared memory: lanes read different entries, which constant memory would
+// serialise.  Warp-uniform result.
+template <class M>
+__device__ __forceinline__ bool self_row_hits(const float4* sp, const short (*bound)[2], const short* begin,
+                                              const unsigned char (*pairs)[2], int stride) {
+    constexpr int NG = M::num_self_groups;
+    const int lane = threadIdx.x & 31;
+    bool hit = false;
+    for (int g0 = 0; g0 < NG && !hit; g0 += 32) {
+        const int g = g0 + lane;
+        const bool gate = g < NG && self_hit(sp[bound[g][0] * stride], sp[bound[g][1] * stride]);
+        uint32_t gm = __ballot_sync(kFull, gate);
+        while (gm && !hit) {
+            const int gg = g0 + __ffs(gm) - 1;
+            gm &= gm - 1u;
+            const int end = begin[gg + 1];
+            for (int k0 = begin[gg]; k0 < end && !hit; k0 += 32) {  // warp-uniform trip count
+                const int k = k0 + lane;
+                const bool h = k < end && self_hit(sp[pairs[k][0] * stride], sp[pairs[k][1] * stride]);
+                hit = __any_sync(kFull, h);
+            }
+        }
+    }
+    return hit;
+}
+
+// One warp per sample row (robots with tiled tables; row-major tables are
+// checked inside fk_staged_kernel), rows strided over the grid, each row by
+// self_row_hits.  Rows of an edge already known to self-collide are skipped.
 constexpr int kSelfThreads = 256;
 
 template <class M>
@@ -270,22 +334,7 @@ __global__ void __launch_bounds__(kSelfThreads) self_kernel(const float4* __rest
         int decided = lane == 0 ? *(volatile const int*)(edge_self + e) : 0;
         if (__shfl_sync(kFull, decided, 0)) continue;  // another row already found a self-collision
         const float4* sp = table + table_index<M>(row, 0);  // sphere s at sp[s * M::table_tile]
-        bool hit = false;
-        for (int g0 = 0; g0 < NG && !hit; g0 += 32) {
-            const int g = g0 + lane;
-            const bool gate = g < NG && self_hit(sp[s_bound[g][0] * M::table_tile], sp[s_bound[g][1] * M::table_tile]);
-            uint32_t gm = __ballot_sync(kFull, gate);
-            while (gm && !hit) {
-                const int gg = g0 + __ffs(gm) - 1;
-                gm &= gm - 1u;
-                const int end = s_begin[gg + 1];
-                for (int k0 = s_begin[gg]; k0 < end && !hit; k0 += 32) {  // warp-uniform trip count
-                    const int k = k0 + lane;
-                    const bool h = k < end && self_hit(sp[s_pairs[k][0] * M::table_tile], sp[s_pairs[k][1] * M::table_tile]);
-                    hit = __any_sync(kFull, h);
-                }
-            }
-        }
+        const bool hit = self_row_hits<M>(sp, s_bound, s_begin, s_pairs, M::table_tile);
         if (hit && lane == 0) atomicOr(edge_self + e, 1);
     }
 }
@@ -1906,30 +1955,40 @@ cudaError_t run_prep(const PipelineArgs& a, cudaStream_t st) {
     const int R = a.total_rows;
     cudaEvent_t* ev = a.stage_events;
     if (ev) cudaEventRecord(ev[1], st);
+    cudaError_t err = cudaMemsetAsync(a.edge_self, 0, sizeof(int) * E, st);
+    if (err != cudaSuccess) return err;
     if (R > 0) {
         if constexpr (M::table_tile == 1) {
+            // FK and self-collision in one kernel; a grid of the resident CTAs
+            // strides over the 32-row blocks
             const size_t smem = 32 * (size_t)(M::num_spheres | 1) * sizeof(float4);
-            cudaError_t err = cudaFuncSetAttribute(fk_staged_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem);
+            err = cudaFuncSetAttribute(fk_staged_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (err != cudaSuccess) return err;
-            fk_staged_kernel<M><<<(R + 31) / 32, 32, smem, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge,
-                                                                  a.fk_perm);
+            int dev = 0, sms = 0, per_sm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk_staged_kernel<M>, 32, smem);
+            if (err != cudaSuccess) return err;
+            const int blocks = (R + 31) / 32;
+            const int grid = std::min(blocks, std::max(per_sm, 1) * std::max(sms, 1));
+            fk_staged_kernel<M><<<grid, 32, smem, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge, a.fk_perm,
+                                                        a.edge_self);
         } else {
             fk_kernel<M><<<(R + 127) / 128, 128, 0, st>>>(a.d_edges, E, a.steps, a.offs, a.table, a.row_edge,
                                                            a.fk_perm);
         }
     }
     if (ev) cudaEventRecord(ev[2], st);
-    cudaError_t err = cudaMemsetAsync(a.edge_self, 0, sizeof(int) * E, st);
-    if (err != cudaSuccess) return err;
-    if (R > 0) {
-        // one warp per row; a grid of at most 16 CTAs per SM strides over the rows
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const long long want = ((long long)R * 32 + kSelfThreads - 1) / kSelfThreads;
-        const int grid = (int)std::min<long long>(want, 16ll * std::max(sms, 1));
-        self_kernel<M><<<grid, kSelfThreads, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
+    if constexpr (M::table_tile != 1) {  // row-major tables: checked by fk_staged_kernel
+        if (R > 0) {
+            // one warp per row; a grid of at most 16 CTAs per SM strides over the rows
+            int dev = 0, sms = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            const long long want = ((long long)R * 32 + kSelfThreads - 1) / kSelfThreads;
+            const int grid = (int)std::min<long long>(want, 16ll * std::max(sms, 1));
+            self_kernel<M><<<grid, kSelfThreads, 0, st>>>(a.table, R, a.row_edge, a.edge_self);
+        }
     }
     if (ev) cudaEventRecord(ev[3], st);
     swept_kernel<M><<<(E * 32 + 255) / 256, 256, 0, st>>>(a.table, a.offs, E, a.swept,

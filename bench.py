@@ -318,6 +318,12 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def plain_launches(robot):
+    """Kernel launches of one plain-order check: Panda's row-major sample table
+    has its self-collision check fused into the FK kernel."""
+    return 5 if robot == "panda" else 6
+
+
 TRAIN_QUEUE_MIN_ITEMS = 128  # the lowest queue threshold the tuner tries: its population holds every higher one's
 
 
@@ -624,7 +630,10 @@ def run_ours(args, world, rank, local, dist):
             "verdict_mismatches_learned_vs_plain": mismatch,
             "proposal": dict(proposal, scored_segments_per_step=learned_rows, queued_pairs_per_step=learned_pairs,
                              queued_fraction=learned_pairs / float(N * E), ranking=ranking),
-            "gpu_launches": (6 + 9 + 9) * args.steps,  # plain: 6 launches per step; learned and its ablation: 9
+            # plain: steps, scan, FK (+ self-collision for row-major tables), [self,]
+            # swept, check; learned adds features, MLP and ranking; its ablation
+            # launches the same
+            "gpu_launches": (3 * plain_launches(robot) + 2 * 3) * args.steps,
             "clocks": clk.summary()}
     line["e2e"] = {"value": world * N * E / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(edges.nbytes),
                    "d2h_bytes_per_step": int(N * E),
