@@ -41,6 +41,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -64,6 +65,16 @@ struct DevTables {
     int self_bound[M::num_self_groups][2];
     int self_pair_begin[M::num_self_groups + 1];
     unsigned char self_pairs[M::num_self_pairs][2];
+    // Self groups whose leaf pairs are every leaf of side 0 against every leaf
+    // of side 1 (self_prod[g] = 1; at most 32 leaves a side, each side's leaves
+    // rigid with its bound): the sides' leaves (row positions) and, per side,
+    // how far its leaves may reach outside its bound plus a margin for FP32
+    // rounding.  A leaf that misses the other side's bound grown by that side's
+    // pad misses every leaf of that side.
+    unsigned char self_prod[M::num_self_groups];
+    int self_la_begin[M::num_self_groups + 1], self_lb_begin[M::num_self_groups + 1];
+    unsigned char self_la[M::num_self_pairs], self_lb[M::num_self_pairs];
+    float self_pad[M::num_self_groups][2];
     float sphere_radius[M::num_spheres];  // by sample-table position
     float s_m[M::dof], s_a[M::dof];       // joint-limit scale q = u * s_m + s_a
 };
@@ -71,6 +82,58 @@ struct DevTables {
 // Specialised by the robot's translation unit to return its __constant__ tables.
 template <class M>
 __device__ __forceinline__ const DevTables<M>& tab();
+
+// Margin (m) added to a side's containment excess in the self groups' leaf
+// filter: far above the FP32 rounding of FK-computed centres (~1e-6 m).
+constexpr double kSelfFilterMargin = 1e-4;
+
+template <class M>
+void self_products(DevTables<M>& t) {
+    int na_tot = 0, nb_tot = 0;
+    for (int g = 0; g < M::num_self_groups; ++g) {
+        const int k0 = M::self_pair_begin[g], k1 = M::self_pair_begin[g + 1];
+        int la[M::num_spheres], lb[M::num_spheres], na = 0, nb = 0;
+        bool in_a[M::num_spheres] = {}, in_b[M::num_spheres] = {};
+        for (int k = k0; k < k1; ++k) {
+            const int a = M::self_pairs[k][0], b = M::self_pairs[k][1];
+            if (!in_a[a]) { in_a[a] = true; la[na++] = a; }
+            if (!in_b[b]) { in_b[b] = true; lb[nb++] = b; }
+        }
+        // a product: as many distinct pairs as |A| x |B| (each pair is in A x B)
+        bool prod = na <= 32 && nb <= 32 && na * nb == k1 - k0;
+        for (int k = k0; k < k1 && prod; ++k)
+            for (int k2 = k0; k2 < k; ++k2)
+                if (M::self_pairs[k2][0] == M::self_pairs[k][0] && M::self_pairs[k2][1] == M::self_pairs[k][1])
+                    prod = false;
+        for (int side = 0; side < 2 && prod; ++side) {
+            const int b = M::self_bound[g][side];
+            double excess = 0.0;
+            for (int i = 0; i < (side ? nb : na); ++i) {
+                const int l = side ? lb[i] : la[i];
+                if (M::sphere_frame[l] != M::sphere_frame[b]) { prod = false; break; }
+                double d2 = 0.0;
+                for (int c = 0; c < 3; ++c) {
+                    const double d = M::sphere_local[l][c] - M::sphere_local[b][c];
+                    d2 += d * d;
+                }
+                const double ex = std::sqrt(d2) + M::sphere_radius[l] - M::sphere_radius[b];
+                excess = ex > excess ? ex : excess;
+            }
+            t.self_pad[g][side] = (float)(excess + kSelfFilterMargin);
+        }
+        t.self_prod[g] = prod ? 1 : 0;
+        t.self_la_begin[g] = na_tot;
+        t.self_lb_begin[g] = nb_tot;
+        if (prod) {
+            for (int i = 0; i < na; ++i) t.self_la[na_tot++] = (unsigned char)M::table_pos[la[i]];
+            for (int i = 0; i < nb; ++i) t.self_lb[nb_tot++] = (unsigned char)M::table_pos[lb[i]];
+        } else {
+            t.self_pad[g][0] = t.self_pad[g][1] = 0.0f;
+        }
+    }
+    t.self_la_begin[M::num_self_groups] = na_tot;
+    t.self_lb_begin[M::num_self_groups] = nb_tot;
+}
 
 template <class M>
 DevTables<M> host_tables() {
@@ -95,6 +158,7 @@ DevTables<M> host_tables() {
         t.self_pairs[i][0] = (unsigned char)M::table_pos[M::self_pairs[i][0]];
         t.self_pairs[i][1] = (unsigned char)M::table_pos[M::self_pairs[i][1]];
     }
+    self_products<M>(t);
     for (int s = 0; s < M::num_spheres; ++s) t.sphere_radius[M::table_pos[s]] = M::sphere_radius[s];
     for (int j = 0; j < M::dof; ++j) {
         t.s_m[j] = M::s_m[j];
@@ -189,22 +253,58 @@ __device__ __forceinline__ bool self_hit(float4 a, float4 b) {
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) - rs * rs < 0.0f;
 }
 
+__device__ __forceinline__ bool self_hit_pad(float4 a, float4 b, float pad) {
+    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    const float rs = a.w + b.w + pad;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) - rs * rs < 0.0f;
+}
+
 // Self-collision of a warp's rows, one lane per row (sphere s at my[s]; live:
 // the lane holds a row), all rows of one edge: group g gates on its bound pair
 // and its leaf pairs count only where the gate hit (the reference's
 // gate-then-leaves).  The warp walks the groups together, so every table index
 // is warp-uniform (constant-cache broadcasts), skips a group's leaves when no
-// lane's gate hit, and stops at the first hit in any lane.  Warp-uniform.
+// lane's gate hit, and stops at the first hit in any lane.  A group whose
+// leaf pairs are a product of two leaf sets (self_prod) first drops the leaves
+// of either side that miss the other side's padded bound -- a leaf of side A
+// that misses bound B (grown by B's containment pad) misses every leaf inside
+// B -- and tests only the pairs of surviving leaves, skipping those no lane
+// keeps; the verdict is the one the full pair list gives.  Warp-uniform.
 template <class M>
 __device__ __forceinline__ bool self_rows_hit(const float4* my, bool live) {
     const DevTables<M>& T = tab<M>();
     for (int g = 0; g < M::num_self_groups; ++g) {
-        const bool gate = live && self_hit(my[T.self_bound[g][0]], my[T.self_bound[g][1]]);
+        const float4 ba = my[T.self_bound[g][0]], bb = my[T.self_bound[g][1]];
+        const bool gate = live && self_hit(ba, bb);
         if (!__any_sync(kFull, gate)) continue;
         bool h = false;
-        const int k1 = T.self_pair_begin[g + 1];
+        if (T.self_prod[g]) {
+            const int a0 = T.self_la_begin[g], na = T.self_la_begin[g + 1] - a0;
+            const int b0 = T.self_lb_begin[g], nb = T.self_lb_begin[g + 1] - b0;
+            const float pa = T.self_pad[g][0], pb = T.self_pad[g][1];
+            uint32_t ma = 0u, mb = 0u;
+            for (int i = 0; i < na; ++i) ma |= (uint32_t)self_hit_pad(my[T.self_la[a0 + i]], bb, pb) << i;
+            for (int j = 0; j < nb; ++j) mb |= (uint32_t)self_hit_pad(my[T.self_lb[b0 + j]], ba, pa) << j;
+            if (!gate || !mb) ma = 0u;
+            uint32_t ia = __reduce_or_sync(kFull, ma);
+            while (ia) {
+                const int i = __ffs(ia) - 1;
+                ia &= ia - 1u;
+                const uint32_t mj = ((ma >> i) & 1u) ? mb : 0u;
+                uint32_t jb = __reduce_or_sync(kFull, mj);
+                const float4 la = my[T.self_la[a0 + i]];
+                while (jb) {
+                    const int j = __ffs(jb) - 1;
+                    jb &= jb - 1u;
+                    h |= ((mj >> j) & 1u) && self_hit(la, my[T.self_lb[b0 + j]]);
+                }
+            }
+        } else {
+            const int k1 = T.self_pair_begin[g + 1];
 #pragma unroll 4
-        for (int k = T.self_pair_begin[g]; k < k1; ++k) h |= self_hit(my[T.self_pairs[k][0]], my[T.self_pairs[k][1]]);
+            for (int k = T.self_pair_begin[g]; k < k1; ++k)
+                h |= self_hit(my[T.self_pairs[k][0]], my[T.self_pairs[k][1]]);
+        }
         if (__any_sync(kFull, gate && h)) return true;
     }
     return false;
