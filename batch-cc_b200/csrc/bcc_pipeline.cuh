@@ -1275,9 +1275,18 @@ __device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, 
         return __ldg(masks + tx * W + w) & __ldg(masks + (kGridTri + ty) * W + w) &
                __ldg(masks + (2 * kGridTri + tz) * W + w);
     };
+    // One mask word (np <= 64, the common case) stays in registers for the
+    // list writes; more words are re-read there.
     int cnt = 0;
-    if (code >= 0)
-        for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
+    uint64_t m1 = 0;
+    if (code >= 0) {
+        if (W == 1) {
+            m1 = mask_word(0);
+            cnt = __popcll(m1);
+        } else {
+            for (int w = 0; w < W; ++w) cnt += __popcll(mask_word(w));
+        }
+    }
     // inclusive scan inside each group of G lanes
     int inc = cnt;
 #pragma unroll
@@ -1304,12 +1313,24 @@ __device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, 
 #pragma unroll
         for (int t = 0; t < SUB; ++t)
             if (t == sub) idx += base[t];
-        for (int w = 0; w < W; ++w) {
-            uint64_t m = mask_word(w);
-            while (m) {
-                const int b = __ffsll((long long)m) - 1;
-                pairs[idx++] = (uint16_t)(((w * 64 + b) << GB) | g);
-                m &= m - 1;
+        if (W == 1) {  // 32-bit halves: cheaper bit steps than 64-bit ones
+            uint32_t lo = (uint32_t)m1, hi = (uint32_t)(m1 >> 32);
+            while (lo) {
+                pairs[idx++] = (uint16_t)(((__ffs((int)lo) - 1) << GB) | g);
+                lo &= lo - 1u;
+            }
+            while (hi) {
+                pairs[idx++] = (uint16_t)(((__ffs((int)hi) + 31) << GB) | g);
+                hi &= hi - 1u;
+            }
+        } else {
+            for (int w = 0; w < W; ++w) {
+                uint64_t m = mask_word(w);
+                while (m) {
+                    const int b = __ffsll((long long)m) - 1;
+                    pairs[idx++] = (uint16_t)(((w * 64 + b) << GB) | g);
+                    m &= m - 1;
+                }
             }
         }
     }
