@@ -555,8 +555,10 @@ __device__ __forceinline__ int learned_rank_to_sample(const uint8_t* perm, int r
 // re-prioritised), starting with sample 0 (where most colliding pairs collide).
 // Each lane holds pi[lane]; the walk fetches pi[r % 32] by shuffle.
 
+// Per-pair walk counts (32 bits: a pair walks at most 32 n C items, far below
+// 2^32; the registers and adds are paid on every walk, counting or not).
 struct WalkStats {
-    unsigned long long chunks = 0, gates = 0, leaf = 0;
+    unsigned chunks = 0, gates = 0, leaf = 0;
 };
 
 // Leaf steps of the overhang-aware walk fetch their item's fields (pair code,
@@ -1016,9 +1018,9 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
     if (MODE == 2) {  // the CTA's warps split the pair: the finish kernel writes the verdict
         if (lane == 0 && P.counters) {
             if (chunk0 == 0) atomicAdd(P.counters + 1, (unsigned long long)C);
-            atomicAdd(P.counters + 2, st.chunks);
-            atomicAdd(P.counters + 3, st.gates);
-            atomicAdd(P.counters + 4, st.leaf);
+            atomicAdd(P.counters + 2, (unsigned long long)st.chunks);
+            atomicAdd(P.counters + 3, (unsigned long long)st.gates);
+            atomicAdd(P.counters + 4, (unsigned long long)st.leaf);
         }
         return;
     }
@@ -1027,9 +1029,9 @@ __device__ __forceinline__ void check_pair(const CheckParams& P, int env, int e,
         if (P.counters) {
             atomicAdd(P.counters + 0, 1ull);
             atomicAdd(P.counters + 1, (unsigned long long)C);
-            atomicAdd(P.counters + 2, st.chunks);
-            atomicAdd(P.counters + 3, st.gates);
-            atomicAdd(P.counters + 4, st.leaf);
+            atomicAdd(P.counters + 2, (unsigned long long)st.chunks);
+            atomicAdd(P.counters + 3, (unsigned long long)st.gates);
+            atomicAdd(P.counters + 4, (unsigned long long)st.leaf);
             atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
         }
     }
@@ -1092,9 +1094,9 @@ __device__ __forceinline__ void walk_listed_pair(const CheckParams& P, int env, 
         if (P.counters) {
             atomicAdd(P.counters + 0, 1ull);
             atomicAdd(P.counters + 1, (unsigned long long)C);
-            atomicAdd(P.counters + 2, st.chunks);
-            atomicAdd(P.counters + 3, st.gates);
-            atomicAdd(P.counters + 4, st.leaf);
+            atomicAdd(P.counters + 2, (unsigned long long)st.chunks);
+            atomicAdd(P.counters + 3, (unsigned long long)st.gates);
+            atomicAdd(P.counters + 4, (unsigned long long)st.leaf);
             atomicAdd(P.counters + 5, collide ? 1ull : 0ull);
         }
     }
@@ -1234,9 +1236,9 @@ __device__ __forceinline__ void walk_halves(const CheckParams& P, int env, int e
             if (P.counters) {
                 atomicAdd(P.counters + 0, 1ull);
                 atomicAdd(P.counters + 1, (unsigned long long)C);
-                atomicAdd(P.counters + 2, st.chunks);
-                atomicAdd(P.counters + 3, st.gates);
-                atomicAdd(P.counters + 4, st.leaf);
+                atomicAdd(P.counters + 2, (unsigned long long)st.chunks);
+                atomicAdd(P.counters + 3, (unsigned long long)st.gates);
+                atomicAdd(P.counters + 4, (unsigned long long)st.leaf);
                 atomicAdd(P.counters + 5, hitp ? 1ull : 0ull);
             }
         }
@@ -1656,9 +1658,9 @@ __global__ void __launch_bounds__(WARPS * 32, finish_min_ctas<M, WARPS>()) finis
                 walk_pairs<M, 2>(P.table, (size_t)P.offs[e], n, C, cta_pairs, prim, np, s_perm[0], 0, GL, undecided,
                                  st, [] { return false; }, 32 * warp, -1, WARPS, &s_hit);
                 if (lane == 0 && P.counters) {
-                    atomicAdd(P.counters + 2, st.chunks);
-                    atomicAdd(P.counters + 3, st.gates);
-                    atomicAdd(P.counters + 4, st.leaf);
+                    atomicAdd(P.counters + 2, (unsigned long long)st.chunks);
+                    atomicAdd(P.counters + 3, (unsigned long long)st.gates);
+                    atomicAdd(P.counters + 4, (unsigned long long)st.leaf);
                 }
             } else if (C < 0) {
                 check_pair<M, 2>(P, env, e, ro, prim, masks, np, W, pairs, s_perm[warp], GL, warp, WARPS, &s_hit);

@@ -317,3 +317,25 @@ def enclosing_sphere(centres_, radii):
             c = 0.5 * (far + near)
             r = 0.5 * np.linalg.norm(near - far)
     return c, r
+
+
+def smallest_enclosing_sphere(centres_, radii):
+    """The smallest sphere containing every (centre, radius) ball: the centre c
+    minimises max_i |c - x_i| + r_i (a convex function), found by Nelder-Mead
+    from three starts; the radius is that maximum at the centre found, so the
+    sphere contains every ball whatever the optimiser's accuracy."""
+    from scipy.optimize import minimize
+
+    pts = np.asarray(centres_, float)
+    r = np.asarray(radii, float)
+
+    def reach(c):
+        return float((np.linalg.norm(pts - c, axis=1) + r).max())
+
+    best = None
+    for start in (pts.mean(0), 0.5 * (pts.min(0) + pts.max(0)), pts[int(np.argmax(r))]):
+        res = minimize(reach, start, method="Nelder-Mead",
+                       options={"xatol": 1e-10, "fatol": 1e-12, "maxiter": 20000})
+        if best is None or reach(res.x) < reach(best):
+            best = res.x
+    return best, reach(best)

@@ -129,8 +129,8 @@ def main():
     w("    static constexpr float sphere_radius[%d] = {%s};" % (
         len(sph), ", ".join(repr(float(np.float32(s["r"]))) + "f" for s in sph)))
     w("")
-    w("    // Environment checks in reference order: group g gates on sphere env_bound[g]")
-    w("    // and then tests leaves env_leaves[env_leaf_begin[g] .. env_leaf_begin[g+1]).")
+    w("    // The checker's environment groups: group g gates on sphere env_bound[g] and")
+    w("    // then tests leaves env_leaves[env_leaf_begin[g] .. env_leaf_begin[g+1]).")
     w("    static constexpr int env_bound[%d] = {%s};" % (len(env), ", ".join(str(g["bound"]) for g in env)))
     begins = [0]
     for g in env:
@@ -145,6 +145,18 @@ def main():
         len(env), ", ".join(str(g.get("over_count", 0)) for g in env)))
     w("    static constexpr float env_cull_pad[%d] = {%s};" % (
         len(env), ", ".join(repr(float(np.float32(g.get("cull_pad", 0.0)))) + "f" for g in env)))
+    w("")
+    ref = m.get("ref_env_groups", env)
+    w("    // The reference's own environment groups (the oracle walks these); equal to")
+    w("    // the groups above where the checker keeps the reference's grouping.")
+    w("    static constexpr int num_ref_env_groups = %d;" % len(ref))
+    w("    static constexpr int ref_env_bound[%d] = {%s};" % (len(ref), ", ".join(str(g["bound"]) for g in ref)))
+    rb = [0]
+    for g in ref:
+        rb.append(rb[-1] + len(g["leaves"]))
+    w("    static constexpr int ref_env_leaf_begin[%d] = {%s};" % (len(rb), ", ".join(map(str, rb))))
+    w("    static constexpr int ref_env_leaves[%d] = {%s};" % (
+        rb[-1], ", ".join(str(i) for g in ref for i in g["leaves"])))
     w("")
     w("    // Self checks in reference order: group g gates on the bound pair self_bound[g]")
     w("    // and then tests the leaf pairs self_pairs[self_pair_begin[g] .. self_pair_begin[g+1]).")

@@ -12,7 +12,8 @@
  *      lane t (0..31), round i (0..n-1): q = fma(delta, t*n, s) + i * delta,
  *      the i additions done one at a time in FP32 (src/batch_cc.cu:126-128);
  *  - per-configuration check fkcc<Robot> (src/utils.cuh:342-5443 for Panda):
- *      environment groups in order, bounding sphere gate then leaf spheres
+ *      the reference's environment groups (the ref_env_* tables) in order,
+ *      bounding sphere gate then leaf spheres
  *      (:806-1190, link0 never env-checked), then self groups, bound pair gate
  *      then leaf pairs (:1192-5440); any hit = collision;
  *  - environment scan sphere_environment_in_collision (src/utils.cuh:213-245):
@@ -265,11 +266,11 @@ template <class M, class T>
 bool config_collides(const EnvView& e, const float* q) {
     T c[M::num_spheres][3];
     forward_kinematics<M, T>(q, c);
-    for (int g = 0; g < M::num_env_groups; ++g) {
-        int b = M::env_bound[g];
+    for (int g = 0; g < M::num_ref_env_groups; ++g) {
+        int b = M::ref_env_bound[g];
         if (!env_hit<T>(e, c[b][0], c[b][1], c[b][2], T(M::sphere_radius[b]))) continue;
-        for (int k = M::env_leaf_begin[g]; k < M::env_leaf_begin[g + 1]; ++k) {
-            int s = M::env_leaves[k];
+        for (int k = M::ref_env_leaf_begin[g]; k < M::ref_env_leaf_begin[g + 1]; ++k) {
+            int s = M::ref_env_leaves[k];
             if (env_hit<T>(e, c[s][0], c[s][1], c[s][2], T(M::sphere_radius[s]))) return true;
         }
     }
@@ -292,12 +293,12 @@ double config_pen(const EnvView& e, const float* q) {
     forward_kinematics<M, double>(q, c);
     const double ninf = -std::numeric_limits<double>::infinity();
     double best = ninf;
-    for (int g = 0; g < M::num_env_groups; ++g) {
-        int b = M::env_bound[g];
+    for (int g = 0; g < M::num_ref_env_groups; ++g) {
+        int b = M::ref_env_bound[g];
         double gp = env_pen(e, c[b][0], c[b][1], c[b][2], M::sphere_radius[b]);
         double lp = ninf;
-        for (int k = M::env_leaf_begin[g]; k < M::env_leaf_begin[g + 1]; ++k) {
-            int s = M::env_leaves[k];
+        for (int k = M::ref_env_leaf_begin[g]; k < M::ref_env_leaf_begin[g + 1]; ++k) {
+            int s = M::ref_env_leaves[k];
             lp = std::max(lp, env_pen(e, c[s][0], c[s][1], c[s][2], M::sphere_radius[s]));
         }
         best = std::max(best, std::min(gp, lp));
@@ -348,10 +349,10 @@ bool config_flops(const EnvView& e, const float* q, double& flops) {
             }
         return false;
     };
-    for (int g = 0; g < M::num_env_groups; ++g) {
-        if (!scan(M::env_bound[g])) continue;
-        for (int k = M::env_leaf_begin[g]; k < M::env_leaf_begin[g + 1]; ++k)
-            if (scan(M::env_leaves[k])) return true;
+    for (int g = 0; g < M::num_ref_env_groups; ++g) {
+        if (!scan(M::ref_env_bound[g])) continue;
+        for (int k = M::ref_env_leaf_begin[g]; k < M::ref_env_leaf_begin[g + 1]; ++k)
+            if (scan(M::ref_env_leaves[k])) return true;
     }
     auto self = [&](int a, int b) {
         flops += 11.0;
