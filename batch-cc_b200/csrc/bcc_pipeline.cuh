@@ -62,6 +62,9 @@ struct DevTables {
     int leaf_begin[M::num_env_groups + 1];
     int over_count[M::num_env_groups];
     float cull_pad[M::num_env_groups];
+    // Certain-hit radius of env group g (0: none): a primitive whose core lies
+    // within rho + cert_r[g] of the bound's centre is hit by a leaf of g.
+    float cert_r[M::num_env_groups];
     int self_bound[M::num_self_groups][2];
     int self_pair_begin[M::num_self_groups + 1];
     unsigned char self_pairs[M::num_self_pairs][2];
@@ -86,6 +89,37 @@ __device__ __forceinline__ const DevTables<M>& tab();
 // Margin (m) added to a side's containment excess in the self groups' leaf
 // filter: far above the FP32 rounding of FK-computed centres (~1e-6 m).
 constexpr double kSelfFilterMargin = 1e-4;
+
+// Certain-hit radius of an environment group.  Leaf l (rigid with the bound's
+// frame, centre c_l, radius r_l) hits a primitive when the distance from c_l
+// to the primitive's core is below r_l + kEnvInflate + rho, and that distance
+// is at most the bound centre's distance d_b plus |c_l - c_b| (distance to a
+// convex set is 1-Lipschitz).  So d_b < rho + max_l (r_l + kEnvInflate -
+// |c_l - c_b|) proves a leaf hit: the leaf penetrates by more than the margin
+// subtracted here, far above FP32 rounding of FK-computed centres, so the
+// reference's own leaf test (src/utils.cuh:806-1190) finds that hit too.
+constexpr double kCertMargin = 1e-4;
+
+template <class M>
+float cert_radius(int g) {
+    const int b = M::env_bound[g];
+    double best = 0.0;
+    for (int k = M::env_leaf_begin[g]; k < M::env_leaf_begin[g + 1]; ++k) {
+        const int l = M::env_leaves[k];
+        if (M::sphere_frame[l] != M::sphere_frame[b]) continue;  // not rigid with the bound
+        double d2 = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            const double d = M::sphere_local[l][c] - M::sphere_local[b][c];
+            d2 += d * d;
+        }
+        const double v = (double)M::sphere_radius[l] + (double)kEnvInflate - std::sqrt(d2) - kCertMargin;
+        best = v > best ? v : best;
+    }
+    // rounded down to float: the test stays conservative
+    float f = (float)best;
+    if ((double)f > best) f = std::nextafter(f, 0.0f);
+    return f;
+}
 
 template <class M>
 void self_products(DevTables<M>& t) {
@@ -146,6 +180,7 @@ DevTables<M> host_tables() {
         t.env_bound[g] = M::env_bound[g];
         t.over_count[g] = M::env_over_count[g];
         t.cull_pad[g] = M::env_cull_pad[g];
+        t.cert_r[g] = cert_radius<M>(g);
     }
     for (int g = 0; g <= M::num_env_groups; ++g) t.leaf_begin[g] = M::env_leaf_begin[g];
     // Self tables hold sample-table row positions, not sphere indices.
@@ -576,6 +611,7 @@ constexpr bool pack_overhang_leaf() {
 // lane-dependent group serialises the access once per distinct group.
 struct GroupLanes {
     int fc;
+    float cert;  // lane g: group g's certain-hit radius
 };
 
 template <class M>
@@ -585,6 +621,7 @@ __device__ __forceinline__ GroupLanes group_lanes() {
     const int first = T.leaf_begin[g];
     GroupLanes r;
     r.fc = first | ((T.leaf_begin[g + 1] - first) << 16);
+    r.cert = T.cert_r[g];
     return r;
 }
 
@@ -654,7 +691,7 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 if (lane == 0) s = *stop;
                 if (__shfl_sync(kFull, s, 0)) break;
             }
-            bool gate = false;
+            bool gate = false, cert = false;
             int g = 0, p = 0, k = 0, cnt = 0, first = 0;
             if constexpr (!kOver) {
                 // c < C on every lane, also past the last item: the pair is decoded and
@@ -665,6 +702,7 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 g = (int)(pr & ((1u << GB) - 1u));
                 p = (int)(pr >> GB);
                 const int fc = __shfl_sync(kFull, GL.fc, g);
+                const float cr = __shfl_sync(kFull, GL.cert, g);
                 first = fc & 0xffff;
                 const int gcnt = fc >> 16;
                 const int blk = block_of(r);
@@ -672,7 +710,13 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                     k = sample_of(r, blk);
                     float4 bs = table[table_index<M>(row0 + (size_t)k, g)];
                     bs.w += kEnvInflate;
-                    gate = sphere_hits_prim(bs, prim + p * kPrimF4);
+                    float rho;
+                    const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
+                    const float rr = bs.w + rho;
+                    gate = d2 - rr * rr < 0.0f;
+                    // the bound's centre close enough to the core proves a leaf hit
+                    const float rc = rho + cr;
+                    cert = cr > 0.0f && d2 - rc * rc < 0.0f;
                     cnt = gate ? gcnt : 0;
                 }
             } else {
@@ -702,6 +746,12 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 first = T.leaf_begin[g];
             }
             ++st.chunks;
+            if constexpr (!kOver) {
+                if (__any_sync(kFull, cert)) {  // a leaf hit is certain: no leaf step
+                    collide = true;
+                    break;
+                }
+            }
             if (__any_sync(kFull, cnt > 0)) {
                 ++st.gates;
                 int incl = cnt;
