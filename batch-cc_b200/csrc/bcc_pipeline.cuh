@@ -107,6 +107,9 @@ float cert_radius(int g) {
     for (int k = M::env_leaf_begin[g]; k < M::env_leaf_begin[g + 1]; ++k) {
         const int l = M::env_leaves[k];
         if (M::sphere_frame[l] != M::sphere_frame[b]) continue;  // not rigid with the bound
+        // r_l <= r_b keeps the radius within r_b + kEnvInflate, so a certain hit
+        // is also a bound hit (the reference tests leaves only after one)
+        if (M::sphere_radius[l] > M::sphere_radius[b]) continue;
         double d2 = 0.0;
         for (int c = 0; c < 3; ++c) {
             const double d = M::sphere_local[l][c] - M::sphere_local[b][c];
@@ -736,6 +739,8 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                     const float d2 = prim_core_d2(bs, prim + p * kPrimF4, &rho);
                     const float rr = bs.w + rho;
                     gate = d2 - rr * rr < 0.0f;
+                    const float rc = rho + T.cert_r[g];
+                    cert = T.cert_r[g] > 0.0f && d2 - rc * rc < 0.0f;
                     cnt = gate ? T.leaf_begin[g + 1] - T.leaf_begin[g] : 0;
                     // overhanging leaves (listed first) near a primitive the bound misses
                     if (!gate && T.over_count[g] > 0) {
@@ -746,11 +751,9 @@ __device__ __forceinline__ bool walk_pairs(const float4* __restrict__ table, siz
                 first = T.leaf_begin[g];
             }
             ++st.chunks;
-            if constexpr (!kOver) {
-                if (__any_sync(kFull, cert)) {  // a leaf hit is certain: no leaf step
-                    collide = true;
-                    break;
-                }
+            if (__any_sync(kFull, cert)) {  // a leaf hit is certain: no leaf step
+                collide = true;
+                break;
             }
             if (__any_sync(kFull, cnt > 0)) {
                 ++st.gates;
