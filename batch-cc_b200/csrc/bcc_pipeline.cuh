@@ -1450,7 +1450,8 @@ __device__ __forceinline__ void check_pair_group(const CheckParams& P, int env, 
 // kernel.  Each warp takes pairs_per_setup consecutive edges at a time.
 template <class M, int WARPS, int MODE>
 __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int tile, int n_slots,
-                                           const unsigned char* smem, float4 h0, float4 h1) {
+                                           const unsigned char* smem, float4 h0, float4 h1,
+                                           int* s_next = nullptr) {
     constexpr int SUB = pairs_per_setup<M>();
     const int e_begin = tile * P.edges_per_cta;
     const int warp = threadIdx.x >> 5;
@@ -1465,7 +1466,24 @@ __device__ __forceinline__ void check_tile(const CheckParams& P, int env, int ti
     uint16_t* pairs =
         reinterpret_cast<uint16_t*>(const_cast<unsigned char*>(smem) + P.blob_smem) + (size_t)warp * P.pairs_per_warp;
     const GroupLanes GL = group_lanes<M>();
-    if constexpr (SUB > 1) {
+    if (s_next) {
+        // Warps take the tile's next pass from a shared counter: a pass costs
+        // from one chunk (a pair colliding at its first sample) to dozens (a
+        // collision-free pair), so a fixed stride leaves warps idle while the
+        // CTA's last one finishes.
+        const int lane = threadIdx.x & 31;
+        for (;;) {
+            int slot = 0;
+            if (lane == 0) slot = atomicAdd(s_next, SUB);
+            slot = __shfl_sync(kFull, slot, 0);
+            if (slot >= n_slots) break;
+            if constexpr (SUB > 1)
+                check_pair_group<M, MODE>(P, env, e_begin + slot, min(SUB, n_slots - slot), prim, masks, np, W,
+                                          pairs, GL);
+            else
+                check_pair<M, MODE>(P, env, e_begin + slot, -1, prim, masks, np, W, pairs, nullptr, GL);
+        }
+    } else if constexpr (SUB > 1) {
         for (int slot = warp * SUB; slot < n_slots; slot += WARPS * SUB)
             check_pair_group<M, MODE>(P, env, e_begin + slot, min(SUB, n_slots - slot), prim, masks, np, W, pairs,
                                       GL);
@@ -1497,12 +1515,14 @@ template <class M, int WARPS, int MODE>
 __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_kernel(CheckParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
+    __shared__ int s_next;
     const int env = blockIdx.x, tile = blockIdx.y;
     const int n_slots = tile_slots(P, tile);
     if (n_slots <= 0) return;
     const float4 h0 = P.env_hdr[2 * env + 0];
     const float4 h1 = P.env_hdr[2 * env + 1];
     const uint32_t bytes = record_bytes_of(h1);
+    if (threadIdx.x == 0) s_next = 0;
     if (bytes) {
         if (threadIdx.x == 0) {
             mbar_init(&bar, 1);
@@ -1518,8 +1538,10 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
             mbar_wait_bounded(&bar, 0u, 1u << 22);
             return;
         }
+    } else {
+        __syncthreads();  // s_next is set before any warp takes a pass
     }
-    check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, h0, h1);
+    check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, h0, h1, &s_next);
 }
 
 // Persistent: a grid sized to the resident capacity pulls environment-major
