@@ -1554,6 +1554,7 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ int s_item;
+    __shared__ int s_next[kItemsPerGrab];  // per grabbed item: the next pass a warp takes
     const int tiles = (P.num_edges + P.edges_per_cta - 1) / P.edges_per_cta;
     const long long items = (long long)P.num_envs * tiles;
     if (threadIdx.x == 0) {
@@ -1564,7 +1565,10 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
     int staged = -1;
     uint32_t phase = 0;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(P.work_counter, kItemsPerGrab);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(P.work_counter, kItemsPerGrab);
+            for (int i = 0; i < kItemsPerGrab; ++i) s_next[i] = 0;
+        }
         __syncthreads();
         const int first = s_item;
         __syncthreads();
@@ -1592,7 +1596,7 @@ __global__ void __launch_bounds__(WARPS * 32, check_min_ctas<M, WARPS>()) check_
                 }
                 staged = env;
             }
-            check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, h0, h1);
+            check_tile<M, WARPS, MODE>(P, env, tile, n_slots, smem, h0, h1, &s_next[item - first]);
         }
         if (failed) break;
         __syncthreads();
