@@ -318,6 +318,18 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def tune_edges(E, N):
+    """Edges the autotuner times a configuration on: all of them up to 10 000,
+    at most ~6e7 (env, edge) pairs per timed check, and at least 5000 edges
+    when there are that many, so that the subset's sample table outgrows the
+    126 MB L2 as the full one does (an L2-resident table favours the persistent
+    kernel's environment-major order, which re-reads the table per environment
+    once it does not fit: on the stress workload a tuning run on 2000 edges
+    picked the persistent kernel, 729 ms per check, where an earlier run's grid
+    kernel took 624 ms)."""
+    return min(E, 10000, max(5000, 60_000_000 // max(N, 1)))
+
+
 def plain_launches(robot):
     """Kernel launches of one plain-order check: Panda's row-major sample table
     has its self-collision check fused into the FK kernel."""
@@ -430,7 +442,7 @@ def measure_workload(chk, name, steps, warmup, flush, dev, parity, train_envs=20
     d_edges = torch.from_numpy(edges).to(f"cuda:{dev}")
     d_res = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
     d_res2 = torch.empty((E, N), dtype=torch.uint8, device=f"cuda:{dev}")
-    n_tune = min(E, 10000, max(1000, 20_000_000 // max(N, 1)))
+    n_tune = tune_edges(E, N)
     tuned = {o: chk.autotune(edges[:n_tune], order=o, robot=robot) for o in ("plain", "learned")}
     ms = {}
     for order, res in (("plain", d_res), ("learned", d_res2)):
@@ -531,8 +543,7 @@ def run_ours(args, world, rank, local, dist):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
 
     # Autotuned launch configuration per order (untimed), on the first edges.
-    # tuning subset: all edges up to 10 000, at most ~2e7 pairs per timed check
-    n_tune = min(E, 10000, max(1000, 20_000_000 // max(N, 1)))
+    n_tune = tune_edges(E, N)
     tuned = {o: chk.autotune(edges[:n_tune], order=o, robot=robot) for o in ("plain", "learned")}
     if dist:
         dist.barrier()
