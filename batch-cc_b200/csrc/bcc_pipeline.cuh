@@ -515,11 +515,25 @@ __global__ void swept_kernel(const float4* __restrict__ table, const int* __rest
     const DevTables<M>& T = tab<M>();
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     if constexpr (M::table_tile == 1) {
-        if (lane < G) {
-            for (int r = r0; r < r1; ++r) {
-                const float4 c = table[table_index<M>(r, lane)];  // bounds lead every table row
+        // 32 / G row streams: lane s G + g scans group g's bound on rows
+        // r0 + s, r0 + s + 32 / G, ... (bounds lead every table row); lane g then
+        // folds in the other streams' boxes.
+        constexpr int RS = kLanes / G;
+        const int rs = lane / G, gl = lane - rs * G;
+        if (rs < RS) {
+            for (int r = r0 + rs; r < r1; r += RS) {
+                const float4 c = table[table_index<M>(r, gl)];
                 lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
                 hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
+            }
+        }
+#pragma unroll
+        for (int t = 1; t < RS; ++t) {
+            const int src = min(lane + t * G, kLanes - 1);  // lanes >= G read a valid lane and discard it
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fminf(lo[a], __shfl_sync(kFull, lo[a], src));
+                hi[a] = fmaxf(hi[a], __shfl_sync(kFull, hi[a], src));
             }
         }
     } else {
