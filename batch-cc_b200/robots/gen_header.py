@@ -36,16 +36,17 @@ FK_FLOPS = {"panda": 1150, "fetch": 983, "baxter": 1792}
 # Rows per tile of the sample table (sphere-major inside a tile): 32 makes the FK
 # kernel's stores coalesced, 1 keeps each row contiguous for the check kernel's
 # bound and leaf reads.  Measured on B200: tiling speeds up the Fetch and Baxter
-# checks (126 / 107 spheres per row, FP64 FK) by 5-6 % and slows Panda's (70
-# spheres, a check dominated by its walk) by 6 %.
+# checks (126 / 107 spheres per row, FP64 FK) by 5-6 % and slowed Panda's (70
+# spheres at the time, a check dominated by its walk) by 6 %.
 TABLE_TILE = {"panda": 1, "fetch": 32, "baxter": 32}
 
 # Resident warps per SM the check kernel is compiled for (its register budget
 # is 65536 / (32 x this)).  Swept on B200 (uneven / multi workloads, autotuned
-# launch shapes): Panda 48 (42 registers) beats 40 by 2 % and 32 by 10 %;
-# Fetch's overhang-aware walk is best at 32 (64 registers); Baxter's at 28
-# (73 registers, 4-warp CTAs) beats 32 by 3 %.
-CHECK_WARPS_PER_SM = {"panda": 48, "fetch": 32, "baxter": 28}
+# launch shapes): Panda 48 (40 registers) beats 40 and 56; Fetch's
+# overhang-aware walk, re-swept with the certain-hit test and the shared pass
+# counter, is best at 40 (48 registers: 1.85 ms against 1.90 at 32 and 2.16 at
+# 24); Baxter's at 28 (72 registers: 3.12 ms against 3.13 at 32, 3.28 at 24).
+CHECK_WARPS_PER_SM = {"panda": 48, "fetch": 40, "baxter": 28}
 
 
 def rpy_matrix(r, p, y):
