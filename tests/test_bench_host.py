@@ -29,3 +29,16 @@ def test_committed_counts_parse():
         assert c[k] > 0, k
     assert 100 < c["inst_per_pair"] < 5000
     assert bench.committed_counts("no_such_workload") is None
+
+
+def test_tuning_subset_outgrows_l2_like_the_full_workload():
+    """The autotuner times configurations on all edges of the benchmark and the
+    configs[2] workloads, and on enough edges of the stress workload that its
+    sample table (about 43 KB of rows per Panda edge) exceeds the 126 MB L2."""
+    bench = _bench()
+    assert bench.tune_edges(10000, 1000) == 10000      # uneven Panda benchmark
+    assert bench.tune_edges(5000, 500) == 5000         # Fetch / Baxter, 500 x 5000
+    n = bench.tune_edges(100000, 10000)                # stress, 10 000 x 100 000
+    assert 5000 <= n <= 10000
+    assert n * 32 * 1.1 * 77 * 16 > 126e6
+    assert bench.tune_edges(300, 10) == 300            # small cases: every edge
