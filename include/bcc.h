@@ -183,10 +183,12 @@ bcc_status bcc_check_noalloc(bcc_robot robot, const float* d_records, const int3
 
 /*
  * Collision-likelihood MLP of the learned check order (no reference
- * counterpart; the north-star learned proposal).  Input row: 48 BF16 features
- * (7 joints normalised to [-1, 1] by the joint limits, 32-value environment
- * code, 9 zeros); 3 hidden layers of 128 (ReLU); output: one logit
- * (collision likelihood).  Parameters are FP32 masters, flat, in the order
+ * counterpart; it proposes the order in which the exact check visits an
+ * edge's samples).  Input row: 48 BF16 features (the robot's joints
+ * normalised to [-1, 1] by the joint limits, the 32-value environment code,
+ * zeros, the sample's position along its edge in [-1, 1] as feature 46;
+ * feature 47 is the bias input the forward kernel reads as 1); 3 hidden
+ * layers of 128 (ReLU); output: one logit (collision likelihood).  Parameters are FP32 masters, flat, in the order
  * W1[48][128], b1[128], W2[128][128], b2[128], W3[128][128], b3[128], w4[128],
  * b4[1]; the kernels use BF16 copies on tcgen05 tensor cores with FP32
  * accumulation.

@@ -33,7 +33,7 @@ def test_committed_counts_parse():
 
 def test_tuning_subset_outgrows_l2_like_the_full_workload():
     """The autotuner times configurations on all edges of the benchmark and the
-    configs[2] workloads, and on enough edges of the stress workload that its
+    Fetch and Baxter workloads, and on enough edges of the stress workload that its
     sample table (about 43 KB of rows per Panda edge) exceeds the 126 MB L2."""
     bench = _bench()
     assert bench.tune_edges(10000, 1000) == 10000      # uneven Panda benchmark
