@@ -127,3 +127,42 @@ def test_certain_hit_radius_implies_a_leaf_hit(robot):
             assert max(pen) > CERT_MARGIN * 0.999, (g.get("link"), max(pen))
             checked += 1
     assert checked > 1000
+
+
+def _extractor():
+    import sys
+    robots = os.path.join(os.path.dirname(HEADERS), "robots")
+    if robots not in sys.path:
+        sys.path.insert(0, robots)
+    import extract_robot
+    return extract_robot
+
+
+def test_regroup_encloses_leaves_and_rejects_bad_partitions():
+    """The generator's regrouping (robots/extract_robot.py `regroup`) on the
+    reference's Panda groups: new bounds enclose their leaves by at least the
+    margin, groups equal to a reference group keep its bound, and partitions
+    that drop a leaf or span two frames are refused."""
+    X = _extractor()
+    m = cases.robot_model("panda")
+    base = dict(m)
+    base["spheres"] = [{k: s[k] for k in ("frame", "local", "r", "link")} for s in m["spheres"] if s["src"] >= 0]
+    base["env_groups"] = m["ref_env_groups"]
+    base.pop("ref_env_groups")
+    out = X.regroup(base, X.PANDA_CHECK_GROUPS)
+    sph = out["spheres"]
+    assert len(sph) == len(m["spheres"])
+    for s_out, s_model in zip(sph[70:], m["spheres"][70:]):  # the committed bounds are reproducible
+        assert np.allclose(s_out["local"], s_model["local"], atol=1e-9) and s_out["r"] == s_model["r"]
+    for g, want in zip(out["env_groups"], m["env_groups"]):
+        assert g["leaves"] == want["leaves"]
+        b = sph[g["bound"]]
+        for l in g["leaves"]:
+            reach = np.linalg.norm(np.subtract(sph[l]["local"], b["local"])) + sph[l]["r"]
+            assert reach <= b["r"] - 0.9 * X.CHECK_BOUND_MARGIN or g["bound"] < 70, (g["link"], l)
+        if g["bound"] < 70:  # a reference group kept whole keeps the reference's bound
+            assert any(r["bound"] == g["bound"] and r["leaves"] == g["leaves"] for r in m["ref_env_groups"])
+    with pytest.raises(SystemExit):
+        X.regroup(base, X.PANDA_CHECK_GROUPS[:-1])               # a leaf missing
+    with pytest.raises(SystemExit):
+        X.regroup(base, [X.PANDA_CHECK_GROUPS[0] + X.PANDA_CHECK_GROUPS[1]] + X.PANDA_CHECK_GROUPS[2:])  # two frames
